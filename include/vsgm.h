@@ -1,0 +1,154 @@
+/* vsgm_b200 C ABI: B200-native subgraph enumeration/counting.
+ *
+ * The reference (VSGM) has no FFI layer; its operator surface is the
+ * pm_pipeline command line plus the in-process PipelineExecutor class.  Every
+ * entry point below names the reference interface it replaces (file:line within
+ * the reference project).  All functions return 0 on success and a negative code
+ * on failure; vsgm_last_error / vsgm_engine_error give the message.  Nothing here
+ * exits the process.  Plain pointers and sizes only; the caller owns every
+ * buffer it passes in.
+ */
+#ifndef VSGM_H
+#define VSGM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "vsgm_plan.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VSGM_OK 0
+#define VSGM_EINVAL (-1)   /* bad argument */
+#define VSGM_EIO (-2)      /* file error */
+#define VSGM_ECUDA (-3)    /* CUDA runtime error */
+#define VSGM_ENOMEM (-4)   /* HBM budget or host memory exhausted */
+#define VSGM_ETIMEOUT (-5) /* a bounded device wait gave up */
+
+/* Message of the last failed host-side call on this thread. */
+const char* vsgm_last_error(void);
+
+/* ------------------------------------------------------------------ planning */
+
+/* Pattern((PresetPatternType)id, false) + Plan::Optimize
+ * (src/query/pattern.h:31-380, src/query/plan.h:548-561; pm_pipeline -p,
+ * src/app/pattern_matching_pipeline.cu:69,79-80).  id in 0..18. */
+int vsgm_plan_pattern(int pattern_id, vsgm_plan* out);
+
+/* Clique(k) + Plan::Optimize (src/query/clique.h:9-37; pm_pipeline -kc,
+ * src/app/pattern_matching_pipeline.cu:61).  k in 3..7. */
+int vsgm_plan_clique(int k, vsgm_plan* out);
+
+/* Query(n, e, adj) + Plan::Optimize (src/query/query.h:62-78): adj_bits[i] bit j
+ * set iff pattern edge (i, j); the pattern must be connected, n in 2..7. */
+int vsgm_plan_query(int n, const uint8_t* adj_bits, vsgm_plan* out);
+
+/* Graphlet(k)->GetQueries() + Plan::Optimize per query (src/query/graphlet.h:15-136;
+ * pm_pipeline -km, src/app/pattern_matching_pipeline.cu:64-66).  Writes at most cap
+ * plans and the total number of graphlets to *n_out. */
+int vsgm_plan_graphlets(int k, vsgm_plan* out, int cap, int* n_out);
+
+/* The plan of the same query with the search sequence taken from seq[0..n-1]
+ * instead of Plan::GenerateSearchSequence (src/query/plan.h:210-265); every later
+ * table is derived as Plan::Optimize derives it.  The learned planner's hook. */
+int vsgm_plan_reorder(const vsgm_plan* base, const uint8_t* seq, vsgm_plan* out);
+
+/* |Aut(P)| of a planned pattern. */
+uint64_t vsgm_plan_automorphisms(const vsgm_plan* p);
+
+/* ------------------------------------------------------------ graphs and files */
+
+/* Release memory this library allocated for the caller. */
+void vsgm_free(void* p);
+
+/* GraphIO::ReadCSRBinFile (src/graph/graph_io.h:57-100), as one bulk read.
+ * *row_ptrs (V+1 entries) and *cols (E entries) are allocated here: vsgm_free. */
+int vsgm_read_csr_bin(const char* path, uint64_t* V, uint64_t* E, uint64_t** row_ptrs, uint32_t** cols);
+
+/* GraphIO::WriteCSRBinFile (src/graph/graph_io.h:313-339). */
+int vsgm_write_csr_bin(const char* path, uint64_t V, uint64_t E, const uint64_t* row_ptrs, const uint32_t* cols);
+
+/* ViewBinManager::LoadViewBinPartition's file read (src/view/view_bin_manager.h:30-41). */
+int vsgm_read_vbmap(const char* path, uint64_t V, int32_t* bins, int32_t* n_bins);
+int vsgm_write_vbmap(const char* path, uint64_t V, const int32_t* bins, int32_t n_bins);
+
+/* GraphIO::Validate (src/graph/graph_io.h:416-444) minus the dangling-vertex
+ * rule: number of self loops, out-of-range, unsorted or duplicate entries. */
+uint64_t vsgm_csr_defects(uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols);
+
+/* Synthetic inputs (the reference reads SNAP/Friendster files instead).  Output
+ * arrays are allocated here: vsgm_free.  threads <= 0 uses every host core. */
+int vsgm_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed, int threads, uint64_t* V, uint64_t* E,
+                  uint64_t** row_ptrs, uint32_t** cols);
+int vsgm_gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t max_degree, uint64_t seed, int threads, uint64_t* E,
+                      uint64_t** row_ptrs, uint32_t** cols);
+/* connected random pattern (n in [n_min, n_max], edge probability p) from stream
+ * seed at *counter; advances *counter. */
+int vsgm_random_pattern(int n_min, int n_max, double p, uint64_t seed, uint64_t* counter, int* n, uint8_t* adj_bits);
+
+/* ViewBin::Materialize (src/view/view_bin.h:66-142): full-V CSR holding the
+ * adjacency rows of every source with degree >= root_degree (all when 0) and of
+ * every vertex within hop-1 steps of one.  view_row_ptrs has V+1 entries; fails
+ * with VSGM_ENOMEM (and *n_cols set) if more than cols_cap entries are needed. */
+int vsgm_view_materialize(uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, const uint32_t* sources, uint64_t n_sources, int hop,
+                          uint64_t root_degree, int threads, uint64_t* view_row_ptrs, uint32_t* view_cols, uint64_t cols_cap, uint64_t* n_cols);
+
+/* ------------------------------------------------------------------- engine */
+
+typedef struct vsgm_engine vsgm_engine; /* one per host thread per GPU */
+
+/* PipelineExecutor(device_id, graph, plans, max_partitioned_sources_num)
+ * (src/executor/pipeline_executor.h:22-47).  hbm_budget_bytes bounds the
+ * engine's working memory (0 = 90% of free HBM; the reference hard-codes
+ * 10.6 GiB at src/common/meta.h:29-36). */
+int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uint64_t max_sources, uint64_t hbm_budget_bytes, vsgm_engine** out);
+
+/* PipelineExecutor::Transfer (src/executor/pipeline_executor.h:64-81): copy one
+ * view (full-V CSR + its sources) from host memory to the device.  The host
+ * buffers may be reused as soon as the call returns. */
+int vsgm_transfer_view(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n_cols, const uint32_t* sources, uint64_t n_sources);
+
+/* Bind a view already resident in device memory on the engine's device (no
+ * copy; the caller keeps it alive until the next transfer or destroy). */
+int vsgm_bind_view_device(vsgm_engine* e, const uint64_t* d_row_ptrs, const uint32_t* d_cols, uint64_t n_cols, const uint32_t* d_sources, uint64_t n_sources);
+
+/* PipelineExecutor::Match (src/executor/pipeline_executor.h:83-109): run every
+ * plan over every source of the current view and add to the per-plan totals. */
+int vsgm_match(vsgm_engine* e);
+
+/* PipelineExecutor::GetTotalCounts (src/executor/pipeline_executor.h:62):
+ * n_plans exact uint64 totals accumulated since create / reset. */
+int vsgm_get_counts(vsgm_engine* e, uint64_t* out);
+int vsgm_reset_counts(vsgm_engine* e);
+
+/* Per-plan execution statistics of the last vsgm_match (no reference
+ * counterpart; the reference prints timings only). */
+typedef struct vsgm_plan_stats {
+  uint64_t op_paths[VSGM_MAX_OPS];    /* partial matches entering each op */
+  uint64_t op_outputs[VSGM_MAX_OPS];  /* candidates / children / count produced */
+  double op_ms[VSGM_MAX_OPS];         /* device time per op (CUDA events) */
+  uint64_t op_launches[VSGM_MAX_OPS]; /* kernels launched per op */
+  uint64_t op_bytes[VSGM_MAX_OPS];    /* algorithmic bytes per op */
+  uint64_t batches;                   /* memory-bounded batches executed */
+  uint64_t peak_bytes;                /* peak working memory */
+} vsgm_plan_stats;
+int vsgm_get_stats(vsgm_engine* e, int plan, vsgm_plan_stats* out);
+
+/* Collect op_ms / op_bytes (adds CUDA events and a small accounting pass). */
+int vsgm_set_profiling(vsgm_engine* e, int on);
+
+/* Engine stream (cudaStream_t) for callers that order their own work with it. */
+void* vsgm_engine_stream(vsgm_engine* e);
+
+const char* vsgm_engine_error(vsgm_engine* e);
+
+/* ~PipelineExecutor (src/executor/pipeline_executor.h:48-54). */
+int vsgm_destroy(vsgm_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

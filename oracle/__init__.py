@@ -1,0 +1,58 @@
+"""CPU ORACLE (test infrastructure only): ctypes access to oracle/liboracle.so.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
+use this package, and only as the checker or the timed CPU baseline; the product
+never imports it.  See oracle/oracle.c for what each function restates.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if os.path.isdir("/root/reference"):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        for name in ("oracle_count", "oracle_op_paths", "oracle_bruteforce"):
+            getattr(L, name).restype = C.c_uint64
+        _lib = L
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def count(plan, g, sources=None, threads=0):
+    """Restated reference executor: exact count of plan over g's sources."""
+    src = np.arange(g.V, dtype=np.uint32) if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+    return int(lib().oracle_count(C.byref(plan), C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
+                                  _p(src, C.c_uint32), C.c_uint64(len(src)), threads))
+
+
+def op_paths(plan, g, sources=None, threads=0):
+    src = np.arange(g.V, dtype=np.uint32) if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+    out = (C.c_uint64 * 24)()
+    total = lib().oracle_op_paths(C.byref(plan), C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
+                                  _p(src, C.c_uint32), C.c_uint64(len(src)), threads, out)
+    return int(total), [int(out[i]) for i in range(plan.n_ops)]
+
+
+def bruteforce(plan, g, n_automorphisms, threads=0):
+    """Injective edge-preserving maps of the pattern into g divided by |Aut(P)|."""
+    return int(lib().oracle_bruteforce(C.byref(plan), C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
+                                       C.c_uint64(n_automorphisms), threads))

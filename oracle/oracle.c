@@ -1,0 +1,328 @@
+/* CPU ORACLE - test infrastructure only.
+ *
+ * Nothing in the product links, imports or executes this file.  It is used by
+ * tests/ (as the checker), by __graft_entry__.smoke() and by bench.py's CPU
+ * baseline / reference arm.
+ *
+ * 1. oracle_count: a restatement of the reference executor for one plan, one
+ *    view (CSR) and its sources.  The reference runs the execution sequence
+ *    level by level over memory-bounded batches; batching never changes a
+ *    count, and every op acts on each partial match independently, so this
+ *    restatement walks the same sequence depth-first per root, with the same
+ *    per-path semantics:
+ *      MATERIALIZE at level 0  src/executor/ops/materialize.h:11-18
+ *      COMPUTE                 src/executor/ops/compute.h:7-41 and the GPSM
+ *                              traversal src/gpu/gpu_utils_gpsm_bin_search.h:14-130
+ *                              (pivot = backward neighbour of least degree,
+ *                              src/gpu/gpu_check_constraints_common.h:11-29;
+ *                              membership by lower-bound search, :32-53 and
+ *                              src/gpu/gpu_utils_bin_search.h:17-29)
+ *      MATERIALIZE             src/executor/ops/materialize.h:20-126
+ *      FILTER_COMPUTE          src/executor/ops/filter_compute.h:14-127
+ *      COMPUTE_COUNT           src/executor/ops/compute_count.h:9-84 with
+ *                              ThreadCountWithComputedVertex
+ *                              src/gpu/gpu_check_constraints_common.h:120-139
+ *      COUNT                   src/executor/ops/count.h:16-167
+ *      conditions              src/gpu/gpu_utils_filter.h:11-23
+ *    OpenMP parallelises over roots.
+ * 2. oracle_bruteforce: independent ground truth - injective edge-preserving
+ *    maps P -> G divided by |Aut(P)|; small graphs only.
+ * 3. oracle_op_paths: number of partial matches entering every op (summed over
+ *    roots), used to check the engine's per-level statistics.
+ *
+ * Parity: the reference's matching path cannot be built here (its moderngpu and
+ * MPMCQueue submodules are not vendored and it needs a GPU), and the reference
+ * ships no golden counts.  This restatement is pinned instead by the brute-force
+ * counter and by closed forms in tests/test_oracle.py; the plans it executes are
+ * pinned to the reference planner's own output (tests/golden/ref_plans.jsonl).
+ */
+#include <omp.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "vsgm_plan.h"
+
+typedef struct {
+  const uint64_t* rp;
+  const uint32_t* ci;
+  const vsgm_plan* p;
+  uint32_t M[VSGM_MAX_QV];
+  const uint32_t* cand[VSGM_MAX_QV];
+  uint64_t clen[VSGM_MAX_QV];
+  uint32_t* buf[VSGM_MAX_OPS]; /* one candidate buffer per op */
+  uint64_t total;
+  uint64_t* op_paths; /* optional per-op partial-match counter */
+} walk_t;
+
+static uint64_t lower_bound_u32(const uint32_t* a, uint64_t n, uint32_t x) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) / 2;
+    if (a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+static int cond_holds(uint8_t op, uint32_t a, uint32_t b) {
+  switch (op) {
+    case VSGM_LESS_THAN: return a < b;
+    case VSGM_LARGER_THAN: return a > b;
+    case VSGM_NON_EQUAL: return a != b;
+    default: return 1;
+  }
+}
+
+static int conds_hold(const vsgm_conds* c, const uint32_t* M, uint32_t x) {
+  for (int i = 0; i < c->count; i++)
+    if (!cond_holds(c->op[i], x, M[c->v[i]])) return 0;
+  return 1;
+}
+
+/* candidates of u: members of N(M[pivot]) adjacent to every other backward
+ * neighbour and satisfying the compute conditions, written to out in order */
+static uint64_t intersect(walk_t* w, int u, uint32_t* out) {
+  const vsgm_plan* p = w->p;
+  const vsgm_vgroup* B = &p->backward[u];
+  int pivot = B->v[0];
+  uint64_t best = w->rp[w->M[pivot] + 1] - w->rp[w->M[pivot]];
+  for (int i = 1; i < B->count; i++) {
+    uint32_t v = w->M[B->v[i]];
+    uint64_t d = w->rp[v + 1] - w->rp[v];
+    if (best > d) {
+      best = d;
+      pivot = B->v[i];
+    }
+  }
+  const uint32_t* list = w->ci + w->rp[w->M[pivot]];
+  uint64_t n = 0;
+  for (uint64_t k = 0; k < best; k++) {
+    uint32_t c = list[k];
+    int ok = 1;
+    for (int i = 0; i < B->count && ok; i++) {
+      if (B->v[i] == pivot) continue;
+      uint32_t v = w->M[B->v[i]];
+      const uint32_t* a = w->ci + w->rp[v];
+      uint64_t len = w->rp[v + 1] - w->rp[v];
+      uint64_t pos = lower_bound_u32(a, len, c);
+      ok = (pos < len && a[pos] == c);
+    }
+    if (ok && conds_hold(&p->compute_cond[u], w->M, c)) out[n++] = c;
+  }
+  return n;
+}
+
+/* elements of a (sorted) that stand in relation op to x, x op a[j] */
+static uint64_t count_vs_set(const uint32_t* a, uint64_t n, uint32_t x, uint8_t op) {
+  if (n == 0) return 0;
+  uint64_t pos = lower_bound_u32(a, n, x);
+  int eq = pos < n && a[pos] == x;
+  if (op == VSGM_LESS_THAN) return n - pos - (eq ? 1 : 0);
+  if (op == VSGM_LARGER_THAN) return pos;
+  return n - (eq ? 1 : 0);
+}
+
+static void run(walk_t* w, int i) {
+  const vsgm_plan* p = w->p;
+  if (i == (int)p->n_ops) return;
+  if (w->op_paths) w->op_paths[i]++;
+  const int u = p->op_vertex[i];
+  switch (p->op_type[i]) {
+    case VSGM_COMPUTE: {
+      uint64_t n = intersect(w, u, w->buf[i]);
+      const uint32_t* old = w->cand[u];
+      uint64_t oldn = w->clen[u];
+      w->cand[u] = w->buf[i];
+      w->clen[u] = n;
+      run(w, i + 1);
+      w->cand[u] = old;
+      w->clen[u] = oldn;
+    } break;
+    case VSGM_MATERIALIZE: {
+      const uint32_t* c = w->cand[u];
+      uint64_t n = w->clen[u];
+      for (uint64_t k = 0; k < n; k++)
+        if (conds_hold(&p->materialize_cond[u], w->M, c[k])) {
+          w->M[u] = c[k];
+          run(w, i + 1);
+        }
+    } break;
+    case VSGM_FILTER_COMPUTE: {
+      const uint32_t* c = w->cand[u];
+      uint64_t n = w->clen[u], m = 0;
+      for (uint64_t k = 0; k < n; k++)
+        if (conds_hold(&p->filter_cond[u], w->M, c[k])) w->buf[i][m++] = c[k];
+      w->cand[u] = w->buf[i];
+      w->clen[u] = m;
+      run(w, i + 1);
+      w->cand[u] = c;
+      w->clen[u] = n;
+    } break;
+    case VSGM_COMPUTE_COUNT: {
+      uint64_t n = intersect(w, u, w->buf[i]);
+      const vsgm_vgroup* um = &p->computed_unmat[i];
+      if (um->count == 0) {
+        w->total += n;
+      } else {
+        int o = um->v[0];
+        uint8_t op = p->order[u][o];
+        for (uint64_t k = 0; k < n; k++) w->total += count_vs_set(w->cand[o], w->clen[o], w->buf[i][k], op);
+      }
+    } break;
+    case VSGM_COUNT: {
+      const vsgm_vgroup* um = &p->computed_unmat[i];
+      if (um->count == 1) {
+        w->total += w->clen[um->v[0]];
+      } else {
+        int u0 = um->v[0], u1 = um->v[1];
+        uint8_t op = p->order[u0][u1];
+        uint64_t n0 = w->clen[u0], n1 = w->clen[u1];
+        /* walk the smaller set, search the larger (src/executor/ops/count.h:16-107) */
+        if (n0 <= n1) {
+          for (uint64_t k = 0; k < n0; k++) w->total += count_vs_set(w->cand[u1], n1, w->cand[u0][k], op);
+        } else {
+          uint8_t rev = op == VSGM_LESS_THAN ? VSGM_LARGER_THAN : (op == VSGM_LARGER_THAN ? VSGM_LESS_THAN : op);
+          for (uint64_t k = 0; k < n1; k++) w->total += count_vs_set(w->cand[u0], n0, w->cand[u1][k], rev);
+        }
+      }
+    } break;
+    default:
+      break;
+  }
+}
+
+static uint64_t max_degree(uint64_t V, const uint64_t* rp) {
+  uint64_t d = 0;
+  for (uint64_t v = 0; v < V; v++)
+    if (rp[v + 1] - rp[v] > d) d = rp[v + 1] - rp[v];
+  return d;
+}
+
+static uint64_t walk_all(const vsgm_plan* p, uint64_t V, const uint64_t* rp, const uint32_t* ci, const uint32_t* sources, uint64_t n_sources,
+                         int threads, uint64_t* op_paths) {
+  const uint64_t dmax = max_degree(V, rp) + 1;
+  const int T = threads > 0 ? threads : omp_get_max_threads();
+  uint64_t total = 0;
+  uint64_t paths[VSGM_MAX_OPS] = {0};
+#pragma omp parallel num_threads(T) reduction(+ : total)
+  {
+    walk_t w;
+    memset(&w, 0, sizeof(w));
+    w.rp = rp;
+    w.ci = ci;
+    w.p = p;
+    uint64_t mine[VSGM_MAX_OPS] = {0};
+    w.op_paths = op_paths ? mine : NULL;
+    for (uint32_t i = 0; i < p->n_ops; i++) w.buf[i] = (uint32_t*)malloc(dmax * sizeof(uint32_t));
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t s = 0; s < (int64_t)n_sources; s++) {
+      w.M[p->op_vertex[0]] = sources[s];
+      if (w.op_paths) mine[0]++;
+      run(&w, 1);
+    }
+    for (uint32_t i = 0; i < p->n_ops; i++) free(w.buf[i]);
+    total += w.total;
+    if (op_paths) {
+#pragma omp critical
+      for (uint32_t i = 0; i < p->n_ops; i++) paths[i] += mine[i];
+    }
+  }
+  if (op_paths)
+    for (uint32_t i = 0; i < p->n_ops; i++) op_paths[i] = paths[i];
+  return total;
+}
+
+uint64_t oracle_count(const vsgm_plan* p, uint64_t V, const uint64_t* rp, const uint32_t* ci, const uint32_t* sources, uint64_t n_sources, int threads) {
+  return walk_all(p, V, rp, ci, sources, n_sources, threads, NULL);
+}
+
+uint64_t oracle_op_paths(const vsgm_plan* p, uint64_t V, const uint64_t* rp, const uint32_t* ci, const uint32_t* sources, uint64_t n_sources, int threads,
+                         uint64_t* op_paths) {
+  return walk_all(p, V, rp, ci, sources, n_sources, threads, op_paths);
+}
+
+/* ---------------------------------------------------------------- brute force */
+typedef struct {
+  const uint64_t* rp;
+  const uint32_t* ci;
+  int n;
+  uint8_t adj[VSGM_MAX_QV];
+  int order[VSGM_MAX_QV]; /* connected visiting order */
+  uint32_t img[VSGM_MAX_QV];
+  uint64_t maps;
+} brute_t;
+
+static int adjacent(const brute_t* b, uint32_t x, uint32_t y) {
+  const uint32_t* a = b->ci + b->rp[x];
+  uint64_t n = b->rp[x + 1] - b->rp[x];
+  uint64_t pos = lower_bound_u32(a, n, y);
+  return pos < n && a[pos] == y;
+}
+
+static void brute(brute_t* b, int k) {
+  if (k == b->n) {
+    b->maps++;
+    return;
+  }
+  int u = b->order[k];
+  /* an earlier-mapped neighbour of u supplies the candidates */
+  int anchor = -1;
+  for (int j = 0; j < k; j++)
+    if (b->adj[u] >> b->order[j] & 1) {
+      anchor = b->order[j];
+      break;
+    }
+  uint32_t a = b->img[anchor];
+  for (uint64_t e = b->rp[a]; e < b->rp[a + 1]; e++) {
+    uint32_t x = b->ci[e];
+    int ok = 1;
+    for (int j = 0; j < k && ok; j++) {
+      int w = b->order[j];
+      if (b->img[w] == x) ok = 0;
+      else if ((b->adj[u] >> w & 1) && w != anchor && !adjacent(b, x, b->img[w])) ok = 0;
+    }
+    if (ok) {
+      b->img[u] = x;
+      brute(b, k + 1);
+    }
+  }
+}
+
+/* injective edge-preserving maps of the pattern into G, divided by |Aut(P)| */
+uint64_t oracle_bruteforce(const vsgm_plan* p, uint64_t V, const uint64_t* rp, const uint32_t* ci, uint64_t n_automorphisms, int threads) {
+  const int n = (int)p->n_vertices;
+  int order[VSGM_MAX_QV];
+  {
+    uint32_t seen = 1;
+    order[0] = 0;
+    for (int k = 1; k < n; k++)
+      for (int u = 0; u < n; u++)
+        if (!(seen >> u & 1) && (p->adj[u] & seen)) {
+          order[k] = u;
+          seen |= 1u << u;
+          break;
+        }
+  }
+  uint64_t maps = 0;
+  const int T = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel num_threads(T) reduction(+ : maps)
+  {
+    brute_t b;
+    memset(&b, 0, sizeof(b));
+    b.rp = rp;
+    b.ci = ci;
+    b.n = n;
+    memcpy(b.adj, p->adj, sizeof(b.adj));
+    memcpy(b.order, order, sizeof(order));
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t v = 0; v < (int64_t)V; v++) {
+      b.img[order[0]] = (uint32_t)v;
+      brute(&b, 1);
+    }
+    maps += b.maps;
+  }
+  return n_automorphisms ? maps / n_automorphisms : 0;
+}

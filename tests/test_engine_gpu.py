@@ -1,0 +1,112 @@
+"""GPU parity: the CUDA engine's exact counts equal the CPU oracle's.
+
+Every test calls the engine through the C ABI (vsgm_create / vsgm_transfer_view
+/ vsgm_match / vsgm_get_counts) and compares with the oracle restatement of the
+reference executor (oracle/oracle.c), itself pinned to brute force in
+tests/test_oracle.py.  Integer counts: the bar is bit-exact equality.
+"""
+import numpy as np
+import pytest
+
+from conftest import all_plans, complete_graph, cycle_graph, empty_graph, small_graphs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def graphs(vs):
+    return small_graphs(vs)
+
+
+@pytest.mark.parametrize("gname", ["rmat7", "rmat8", "chunglu"])
+def test_every_preset_clique_and_graphlet(vs, orc, graphs, gname):
+    g = graphs[gname]
+    plans = all_plans(vs)
+    got = vs.count_graph(g, [p for _, p in plans])
+    want = [orc.count(p, g) for _, p in plans]
+    bad = [(n, w, x) for (n, _), w, x in zip(plans, want, got) if w != x]
+    assert not bad, bad
+
+
+def test_random_patterns(vs, orc, graphs):
+    g = graphs["rmat8"]
+    ctr = 0
+    plans = []
+    for _ in range(48):
+        n, bits, ctr = vs.random_pattern(seed=3, counter=ctr, n_min=3, n_max=6, p=0.5)
+        plans.append(vs.plan_query_bits(n, bits))
+    got = vs.count_graph(g, plans)
+    want = [orc.count(p, g) for p in plans]
+    assert got == want
+
+
+def test_closed_forms(vs):
+    from math import comb
+    k7 = complete_graph(vs, 7)
+    got = vs.count_graph(k7, [vs.plan_clique(k) for k in range(3, 8)])
+    assert got == [comb(7, k) for k in range(3, 8)]
+    c9 = cycle_graph(vs, 9)
+    assert vs.count_graph(c9, [vs.plan_clique(3), vs.plan_pattern(1)]) == [0, 0]
+    c4 = cycle_graph(vs, 4)
+    assert vs.count_graph(c4, [vs.plan_pattern(1)]) == [1]  # exactly one 4-cycle
+    assert vs.count_graph(empty_graph(vs, 16), [vs.plan_clique(3), vs.plan_pattern(2)]) == [0, 0]
+
+
+def test_views_partition_invariance(vs, orc, graphs):
+    """Counts summed over views equal the whole-graph count (src/view/view_bin.h:49-142)."""
+    g = graphs["rmat8"]
+    plans = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2), vs.plan_pattern(4)]
+    whole = vs.count_graph(g, plans)
+    rng = np.random.default_rng(5)
+    bins = rng.integers(0, 4, size=g.V).astype(np.int32)
+    views = vs.sources_of_bins(bins, 4)
+    assert vs.count_graph(g, plans, views=views) == whole
+    assert whole == [orc.count(p, g) for p in plans]
+
+
+def test_tiny_budget_forces_batches(vs, orc, graphs):
+    """Memory-bounded batching must not change a count."""
+    g = graphs["rmat8"]
+    plans = [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(4), vs.plan_pattern(13)]
+    want = [orc.count(p, g) for p in plans]
+    with vs.Engine(g.V, plans, hbm_budget_bytes=1 << 21) as e:
+        e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+        e.match()
+        assert e.counts() == want
+        assert max(e.stats(i).batches for i in range(len(plans))) > 4
+
+
+def test_stats_match_oracle_paths(vs, orc, graphs):
+    g = graphs["rmat7"]
+    for p in [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(3)]:
+        total, paths = orc.op_paths(p, g)
+        with vs.Engine(g.V, [p]) as e:
+            e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+            e.match()
+            assert e.counts() == [total]
+            s = e.stats(0)
+            assert [s.op_paths[i] for i in range(p.n_ops)] == paths
+
+
+def test_counts_accumulate_across_views_and_reset(vs, graphs):
+    g = graphs["rmat7"]
+    p = vs.plan_clique(3)
+    with vs.Engine(g.V, [p]) as e:
+        src = np.arange(g.V, dtype=np.uint32)
+        e.transfer_view(g, src)
+        e.match()
+        one = e.counts()[0]
+        e.match()
+        assert e.counts()[0] == 2 * one
+        e.reset_counts()
+        e.match()
+        assert e.counts()[0] == one
+
+
+def test_engine_rejects_bad_views(vs, graphs):
+    g = graphs["rmat7"]
+    with vs.Engine(g.V, [vs.plan_clique(3)]) as e:
+        with pytest.raises(vs.VsgmError):
+            e.transfer_view(g, np.array([g.V + 5], dtype=np.uint32))
+        with pytest.raises(vs.VsgmError):
+            e.match()  # no view transferred yet

@@ -1,0 +1,68 @@
+"""Pin the CPU oracle before trusting it.
+
+The reference ships no golden counts and its matching path cannot be built here,
+so the restatement of its executor (oracle/oracle.c) is pinned to (a) an
+independent brute-force counter (injective edge-preserving maps / |Aut(P)|) on
+every preset pattern, clique, graphlet and random pattern, and (b) closed forms.
+"""
+from math import comb
+
+import numpy as np
+import pytest
+
+from conftest import all_plans, complete_graph, cycle_graph, empty_graph
+
+
+@pytest.fixture(scope="module")
+def g(vs):
+    return vs.gen_rmat(7, 8, seed=11)
+
+
+def test_restatement_equals_bruteforce_all_named_queries(vs, orc, g):
+    bad = []
+    for name, p in all_plans(vs):
+        a = orc.count(p, g)
+        b = orc.bruteforce(p, g, vs.automorphisms(p))
+        if a != b:
+            bad.append((name, a, b))
+    assert not bad, bad
+
+
+def test_restatement_equals_bruteforce_random_patterns(vs, orc):
+    g = vs.gen_chung_lu(300, 1500, 2.2, 40, seed=2)
+    ctr = 0
+    for _ in range(40):
+        n, bits, ctr = vs.random_pattern(seed=3, counter=ctr, n_min=3, n_max=6)
+        p = vs.plan_query_bits(n, bits)
+        assert orc.count(p, g) == orc.bruteforce(p, g, vs.automorphisms(p)), p.describe()
+
+
+def test_closed_forms(vs, orc):
+    k7 = complete_graph(vs, 7)
+    for k in range(3, 8):
+        assert orc.count(vs.plan_clique(k), k7) == comb(7, k)
+    for n in (4, 5, 6):
+        c = cycle_graph(vs, n)
+        pid = {4: 1, 5: 16, 6: 17}[n]
+        assert orc.count(vs.plan_pattern(pid), c) == 1
+        assert orc.count(vs.plan_clique(3), c) == 0
+    assert orc.count(vs.plan_pattern(2), empty_graph(vs, 10)) == 0
+
+
+def test_automorphism_counts(vs):
+    assert vs.automorphisms(vs.plan_clique(4)) == 24
+    assert vs.automorphisms(vs.plan_pattern(1)) == 8   # 4-cycle
+    assert vs.automorphisms(vs.plan_pattern(2)) == 4   # diamond
+    assert vs.automorphisms(vs.plan_pattern(4)) == 2   # house
+    assert vs.automorphisms(vs.plan_pattern(16)) == 10  # 5-cycle
+
+
+def test_oracle_counts_are_view_invariant(vs, orc, g):
+    p = vs.plan_pattern(4)
+    whole = orc.count(p, g)
+    bins = np.arange(g.V) % 3
+    total = 0
+    for src in vs.sources_of_bins(bins.astype(np.int32), 3):
+        v = vs.materialize_view(g, src, p.hop, p.root_degree)
+        total += orc.count(p, v, src)
+    assert total == whole

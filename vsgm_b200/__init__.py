@@ -1,0 +1,257 @@
+"""vsgm_b200: B200-native subgraph enumeration/counting behind VSGM's pm_pipeline surface.
+
+Python is a thin layer over the C ABI (include/vsgm.h); every count comes from
+the CUDA engine in libvsgm_b200.so.  Names follow the reference:
+
+    plan_pattern(p)       Pattern((PresetPatternType)p, false) + Plan::Optimize
+    plan_clique(k)        Clique(k) + Plan::Optimize                (-kc)
+    plan_graphlets(k)     Graphlet(k)->GetQueries(), planned        (-km)
+    plan_query(adj)       Query(n, e, adj) + Plan::Optimize
+    read_csr_bin / write_csr_bin / read_vbmap                       (src/graph/graph_io.h, src/view)
+    materialize_view      ViewBin::Materialize                      (src/view/view_bin.h:66-142)
+    Engine                PipelineExecutor                          (src/executor/pipeline_executor.h)
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import Plan, PlanStats, VsgmError
+
+__all__ = [
+    "Plan", "PlanStats", "VsgmError", "Graph", "Engine",
+    "plan_pattern", "plan_clique", "plan_query", "plan_graphlets", "plan_reorder", "automorphisms",
+    "gen_rmat", "gen_chung_lu", "random_pattern", "read_csr_bin", "write_csr_bin", "read_vbmap", "write_vbmap",
+    "csr_defects", "materialize_view", "sources_of_bins",
+]
+
+
+def _L():
+    return capi.lib()
+
+
+# ------------------------------------------------------------------ planning
+def plan_pattern(pattern_id):
+    p = Plan()
+    capi.check(_L().vsgm_plan_pattern(int(pattern_id), C.byref(p)))
+    return p
+
+
+def plan_clique(k):
+    p = Plan()
+    capi.check(_L().vsgm_plan_clique(int(k), C.byref(p)))
+    return p
+
+
+def plan_query(neighbours):
+    """Plan of a connected pattern given as neighbour lists (Query(n, e, adj), src/query/query.h:62-78)."""
+    n = len(neighbours)
+    bits = (C.c_uint8 * capi.MAX_QV)()
+    for i, row in enumerate(neighbours):
+        for j in row:
+            bits[i] |= 1 << int(j)
+    p = Plan()
+    capi.check(_L().vsgm_plan_query(n, bits, C.byref(p)))
+    return p
+
+
+def plan_query_bits(n, bits):
+    arr = (C.c_uint8 * capi.MAX_QV)(*[int(b) for b in list(bits)[:capi.MAX_QV]])
+    p = Plan()
+    capi.check(_L().vsgm_plan_query(int(n), arr, C.byref(p)))
+    return p
+
+
+def plan_graphlets(k):
+    arr = (Plan * 64)()
+    n = C.c_int()
+    capi.check(_L().vsgm_plan_graphlets(int(k), arr, 64, C.byref(n)))
+    return [arr[i] for i in range(n.value)]
+
+
+def plan_reorder(base, seq):
+    s = (C.c_uint8 * capi.MAX_QV)(*[int(x) for x in seq])
+    p = Plan()
+    capi.check(_L().vsgm_plan_reorder(C.byref(base), s, C.byref(p)))
+    return p
+
+
+def automorphisms(plan):
+    return int(_L().vsgm_plan_automorphisms(C.byref(plan)))
+
+
+# -------------------------------------------------------------------- graphs
+class Graph:
+    """Undirected CSR: row_ptrs (uint64, V+1), cols (uint32, E = 2 x undirected edges)."""
+
+    def __init__(self, row_ptrs, cols):
+        self.row_ptrs = np.ascontiguousarray(row_ptrs, dtype=np.uint64)
+        self.cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        self.V = len(self.row_ptrs) - 1
+
+    @property
+    def E(self):
+        return len(self.cols)
+
+    def degrees(self):
+        return np.diff(self.row_ptrs)
+
+
+def _take(ptr_u64, ptr_u32, V, E):
+    rp = np.ctypeslib.as_array(ptr_u64, shape=(V + 1,)).copy()
+    ci = np.ctypeslib.as_array(ptr_u32, shape=(max(E, 1),))[:E].copy() if E else np.zeros(0, np.uint32)
+    _L().vsgm_free(C.cast(ptr_u64, C.c_void_p))
+    _L().vsgm_free(C.cast(ptr_u32, C.c_void_p))
+    return Graph(rp, ci)
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=1, threads=0):
+    V, E = C.c_uint64(), C.c_uint64()
+    rp, ci = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+    capi.check(_L().vsgm_gen_rmat(scale, edge_factor, a, b, c, seed, threads, C.byref(V), C.byref(E), C.byref(rp), C.byref(ci)))
+    return _take(rp, ci, V.value, E.value)
+
+
+def gen_chung_lu(V, target_edges, gamma, max_degree, seed, threads=0):
+    E = C.c_uint64()
+    rp, ci = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+    capi.check(_L().vsgm_gen_chung_lu(V, target_edges, gamma, max_degree, seed, threads, C.byref(E), C.byref(rp), C.byref(ci)))
+    return _take(rp, ci, V, E.value)
+
+
+def random_pattern(seed, counter, n_min=3, n_max=6, p=0.5):
+    """Returns (n, adj_bits, next_counter)."""
+    ctr = C.c_uint64(counter)
+    n = C.c_int()
+    bits = (C.c_uint8 * capi.MAX_QV)()
+    capi.check(_L().vsgm_random_pattern(n_min, n_max, p, seed, C.byref(ctr), C.byref(n), bits))
+    return n.value, [bits[i] for i in range(capi.MAX_QV)], ctr.value
+
+
+def read_csr_bin(path):
+    V, E = C.c_uint64(), C.c_uint64()
+    rp, ci = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+    capi.check(_L().vsgm_read_csr_bin(str(path).encode(), C.byref(V), C.byref(E), C.byref(rp), C.byref(ci)))
+    return _take(rp, ci, V.value, E.value)
+
+
+def write_csr_bin(path, g):
+    capi.check(_L().vsgm_write_csr_bin(str(path).encode(), g.V, g.E, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32)))
+
+
+def read_vbmap(path, V):
+    bins = np.zeros(V, np.int32)
+    nb = C.c_int32()
+    capi.check(_L().vsgm_read_vbmap(str(path).encode(), V, capi.ptr(bins, C.c_int32), C.byref(nb)))
+    return bins, nb.value
+
+
+def write_vbmap(path, bins, n_bins):
+    bins = np.ascontiguousarray(bins, dtype=np.int32)
+    capi.check(_L().vsgm_write_vbmap(str(path).encode(), len(bins), capi.ptr(bins, C.c_int32), int(n_bins)))
+
+
+def csr_defects(g):
+    return int(_L().vsgm_csr_defects(g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32)))
+
+
+def sources_of_bins(bins, n_bins):
+    """Per-bin ascending source lists (ViewBinManager::LoadViewBinPartition, src/view/view_bin_manager.h:43-60)."""
+    order = np.argsort(bins, kind="stable").astype(np.uint32)
+    counts = np.bincount(bins, minlength=n_bins)
+    out, at = [], 0
+    for b in range(n_bins):
+        out.append(order[at:at + counts[b]])
+        at += counts[b]
+    return out
+
+
+def materialize_view(g, sources, hop, root_degree=0, threads=0):
+    """Full-V view CSR holding the rows of the sources' (hop-1)-neighbourhood."""
+    sources = np.ascontiguousarray(sources, dtype=np.uint32)
+    vrp = np.zeros(g.V + 1, np.uint64)
+    n = C.c_uint64()
+    cap = g.E
+    vci = np.zeros(max(cap, 1), np.uint32)
+    capi.check(_L().vsgm_view_materialize(g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32),
+                                          capi.ptr(sources, C.c_uint32), len(sources), hop, root_degree, threads,
+                                          capi.ptr(vrp, C.c_uint64), capi.ptr(vci, C.c_uint32), cap, C.byref(n)))
+    return Graph(vrp, vci[:n.value])
+
+
+# -------------------------------------------------------------------- engine
+class Engine:
+    """PipelineExecutor on one GPU: transfer a view, match every plan, read exact counts."""
+
+    def __init__(self, V, plans, device=0, max_sources=0, hbm_budget_bytes=0):
+        self.plans = list(plans)
+        arr = (Plan * len(self.plans))(*self.plans)
+        h = C.c_void_p()
+        capi.check(_L().vsgm_create(device, V, arr, len(self.plans), max_sources, hbm_budget_bytes, C.byref(h)))
+        self.h = h
+        self.V = V
+
+    def transfer_view(self, view, sources):
+        sources = np.ascontiguousarray(sources, dtype=np.uint32)
+        self._keep = (view, sources)
+        capi.check(_L().vsgm_transfer_view(self.h, capi.ptr(view.row_ptrs, C.c_uint64), capi.ptr(view.cols, C.c_uint32),
+                                           view.E, capi.ptr(sources, C.c_uint32), len(sources)), self.h)
+
+    def bind_view_device(self, d_row_ptrs, d_cols, n_cols, d_sources, n_sources):
+        capi.check(_L().vsgm_bind_view_device(self.h, C.c_void_p(d_row_ptrs), C.c_void_p(d_cols), n_cols,
+                                              C.c_void_p(d_sources), n_sources), self.h)
+
+    def match(self):
+        capi.check(_L().vsgm_match(self.h), self.h)
+
+    def counts(self):
+        out = np.zeros(len(self.plans), np.uint64)
+        capi.check(_L().vsgm_get_counts(self.h, capi.ptr(out, C.c_uint64)), self.h)
+        return [int(x) for x in out]
+
+    def reset_counts(self):
+        capi.check(_L().vsgm_reset_counts(self.h), self.h)
+
+    def stats(self, plan=0):
+        s = PlanStats()
+        capi.check(_L().vsgm_get_stats(self.h, plan, C.byref(s)), self.h)
+        return s
+
+    def set_profiling(self, on=True):
+        capi.check(_L().vsgm_set_profiling(self.h, 1 if on else 0), self.h)
+
+    def stream(self):
+        return _L().vsgm_engine_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _L().vsgm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def count_graph(g, plans, sources=None, device=0, hbm_budget_bytes=0, views=None, hop=None):
+    """Exact counts of every plan over g (all vertices as sources, one view), or
+    over a list of per-view source arrays, each materialised with the plans' hop."""
+    with Engine(g.V, plans, device=device, hbm_budget_bytes=hbm_budget_bytes) as e:
+        if views is None:
+            e.transfer_view(g, np.arange(g.V, dtype=np.uint32) if sources is None else sources)
+            e.match()
+        else:
+            h = hop or max(p.hop for p in plans)
+            rd = min(p.root_degree for p in plans)
+            for src in views:
+                e.transfer_view(materialize_view(g, src, h, rd), src)
+                e.match()
+        return e.counts()

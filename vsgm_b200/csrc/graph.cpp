@@ -1,0 +1,300 @@
+// Host-side graph layer (see graph.hpp).
+#include "graph.hpp"
+
+#include <omp.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+
+namespace vsgm {
+
+uint64_t mix64(uint64_t seed, uint64_t i) {
+  // splitmix64 finaliser over a seed-salted counter
+  uint64_t z = seed * 0x9E3779B97F4A7C15ull + i * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+double unit_double(uint64_t seed, uint64_t i) { return (double)(mix64(seed, i) >> 11) * (1.0 / 9007199254740992.0); }
+
+static int nthreads(int t) { return t > 0 ? t : omp_get_max_threads(); }
+
+void csr_from_edges(uint64_t V, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst, int threads, Csr* out) {
+  const int T = nthreads(threads);
+  const uint64_t m = src.size();
+  std::vector<uint64_t> deg(V + 1, 0);
+  {
+    std::atomic<uint64_t>* d = reinterpret_cast<std::atomic<uint64_t>*>(deg.data());
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int64_t i = 0; i < (int64_t)m; i++) {
+      if (src[i] == dst[i]) continue;
+      d[src[i]].fetch_add(1, std::memory_order_relaxed);
+      d[dst[i]].fetch_add(1, std::memory_order_relaxed);
+    }
+  }
+  std::vector<uint64_t> off(V + 1, 0);
+  for (uint64_t v = 0; v < V; v++) off[v + 1] = off[v] + deg[v];
+  std::vector<uint32_t> tmp(off[V]);
+  {
+    std::vector<uint64_t> cur(off.begin(), off.end() - 1);
+    std::atomic<uint64_t>* c = reinterpret_cast<std::atomic<uint64_t>*>(cur.data());
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int64_t i = 0; i < (int64_t)m; i++) {
+      uint32_t a = src[i], b = dst[i];
+      if (a == b) continue;
+      tmp[c[a].fetch_add(1, std::memory_order_relaxed)] = b;
+      tmp[c[b].fetch_add(1, std::memory_order_relaxed)] = a;
+    }
+  }
+  // sort + unique each row in place
+  std::vector<uint64_t> kept(V + 1, 0);
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
+  for (int64_t v = 0; v < (int64_t)V; v++) {
+    uint32_t* b = tmp.data() + off[v];
+    uint32_t* e = tmp.data() + off[v + 1];
+    std::sort(b, e);
+    kept[v] = (uint64_t)(std::unique(b, e) - b);
+  }
+  out->V = V;
+  out->row_ptrs.assign(V + 1, 0);
+  for (uint64_t v = 0; v < V; v++) out->row_ptrs[v + 1] = out->row_ptrs[v] + kept[v];
+  out->cols.resize(out->row_ptrs[V]);
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
+  for (int64_t v = 0; v < (int64_t)V; v++)
+    std::memcpy(out->cols.data() + out->row_ptrs[v], tmp.data() + off[v], kept[v] * sizeof(uint32_t));
+}
+
+void gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed, int threads, Csr* out) {
+  const uint64_t V = 1ull << scale;
+  const uint64_t m = (uint64_t)edge_factor << scale;
+  std::vector<uint32_t> src(m), dst(m);
+  const double ab = a + b, abc = a + b + c;
+#pragma omp parallel for num_threads(nthreads(threads)) schedule(static)
+  for (int64_t i = 0; i < (int64_t)m; i++) {
+    uint64_t s = 0, d = 0;
+    for (int l = 0; l < scale; l++) {
+      double r = unit_double(seed, (uint64_t)i * 64 + l);
+      s <<= 1;
+      d <<= 1;
+      if (r < a) {
+      } else if (r < ab) {
+        d |= 1;
+      } else if (r < abc) {
+        s |= 1;
+      } else {
+        s |= 1;
+        d |= 1;
+      }
+    }
+    src[i] = (uint32_t)s;
+    dst[i] = (uint32_t)d;
+  }
+  csr_from_edges(V, src, dst, threads, out);
+}
+
+void gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t dmax, uint64_t seed, int threads, Csr* out) {
+  const int T = nthreads(threads);
+  const double beta = 1.0 / (gamma - 1.0);
+  // sum of w for offset i0, by direct summation (V up to ~1e8 is fine)
+  auto total = [&](double i0) {
+    double s = 0;
+#pragma omp parallel for num_threads(T) reduction(+ : s)
+    for (int64_t i = 0; i < (int64_t)V; i++) s += (double)dmax * std::pow((i + i0) / i0, -beta);
+    return s;
+  };
+  const double want = 2.0 * (double)target_edges;
+  double lo = 1e-3, hi = (double)V * 4;
+  for (int it = 0; it < 80; it++) {
+    double mid = std::sqrt(lo * hi);
+    if (total(mid) < want)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const double i0 = std::sqrt(lo * hi);
+  std::vector<double> cdf(V);
+  {
+    double s = 0;
+    for (uint64_t i = 0; i < V; i++) {
+      s += (double)dmax * std::pow((i + i0) / i0, -beta);
+      cdf[i] = s;
+    }
+    for (uint64_t i = 0; i < V; i++) cdf[i] /= s;
+    cdf[V - 1] = 1.0;
+  }
+  const uint64_t m = target_edges;
+  std::vector<uint32_t> src(m), dst(m);
+#pragma omp parallel for num_threads(T) schedule(static)
+  for (int64_t i = 0; i < (int64_t)m; i++) {
+    double r1 = unit_double(seed, 2 * (uint64_t)i), r2 = unit_double(seed, 2 * (uint64_t)i + 1);
+    src[i] = (uint32_t)(std::upper_bound(cdf.begin(), cdf.end(), r1) - cdf.begin());
+    dst[i] = (uint32_t)(std::upper_bound(cdf.begin(), cdf.end(), r2) - cdf.begin());
+    if (src[i] >= V) src[i] = (uint32_t)(V - 1);
+    if (dst[i] >= V) dst[i] = (uint32_t)(V - 1);
+  }
+  csr_from_edges(V, src, dst, threads, out);
+}
+
+bool read_csr_bin(const std::string& path, Csr* out, std::string* err) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
+    if (err) *err = "cannot open " + path;
+    return false;
+  }
+  uint64_t hdr[4];
+  bool ok = std::fread(hdr, sizeof(uint64_t), 4, f) == 4;
+  if (ok && (hdr[0] != 4 || hdr[1] != 8)) {
+    if (err) *err = "unsupported id widths in " + path;
+    std::fclose(f);
+    return false;
+  }
+  if (ok) {
+    out->V = hdr[2];
+    out->row_ptrs.resize(hdr[2] + 1);
+    out->cols.resize(hdr[3]);
+    ok = std::fread(out->row_ptrs.data(), sizeof(uint64_t), hdr[2] + 1, f) == hdr[2] + 1;
+    ok = ok && std::fread(out->cols.data(), sizeof(uint32_t), hdr[3], f) == hdr[3];
+    ok = ok && out->row_ptrs[hdr[2]] == hdr[3] && std::fgetc(f) == EOF;
+  }
+  std::fclose(f);
+  if (!ok && err) *err = "truncated or inconsistent csr file " + path;
+  return ok;
+}
+
+bool write_csr_bin(const std::string& path, const Csr& g, std::string* err) {
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    if (err) *err = "cannot create " + path;
+    return false;
+  }
+  uint64_t hdr[4] = {4, 8, g.V, g.E()};
+  bool ok = std::fwrite(hdr, sizeof(uint64_t), 4, f) == 4;
+  ok = ok && std::fwrite(g.row_ptrs.data(), sizeof(uint64_t), g.V + 1, f) == g.V + 1;
+  ok = ok && std::fwrite(g.cols.data(), sizeof(uint32_t), g.E(), f) == g.E();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok && err) *err = "write failed for " + path;
+  return ok;
+}
+
+bool read_vbmap(const std::string& path, uint64_t V, std::vector<int32_t>* bins, int32_t* n_bins, std::string* err) {
+  std::ifstream in(path);
+  if (!in) {
+    if (err) *err = "cannot open " + path;
+    return false;
+  }
+  int64_t nb = 0;
+  in >> nb;
+  bins->assign(V, 0);
+  for (uint64_t i = 0; i < V; i++) {
+    int64_t b;
+    if (!(in >> b) || b < 0 || b >= nb) {
+      if (err) *err = "bad or missing bin id for vertex " + std::to_string(i) + " in " + path;
+      return false;
+    }
+    (*bins)[i] = (int32_t)b;
+  }
+  *n_bins = (int32_t)nb;
+  return true;
+}
+
+bool write_vbmap(const std::string& path, const std::vector<int32_t>& bins, int32_t n_bins, std::string* err) {
+  FILE* f = std::fopen(path.c_str(), "w");
+  if (!f) {
+    if (err) *err = "cannot create " + path;
+    return false;
+  }
+  std::fprintf(f, "%d\n", n_bins);
+  for (int32_t b : bins) std::fprintf(f, "%d\n", b);
+  std::fclose(f);
+  return true;
+}
+
+uint64_t csr_defects(const Csr& g) {
+  uint64_t bad = 0;
+  for (uint64_t v = 0; v < g.V; v++)
+    for (uint64_t j = g.row_ptrs[v]; j < g.row_ptrs[v + 1]; j++) {
+      if (g.cols[j] == v || g.cols[j] >= g.V) bad++;
+      if (j > g.row_ptrs[v] && g.cols[j] <= g.cols[j - 1]) bad++;
+    }
+  return bad;
+}
+
+bool materialize_view(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t V, const uint32_t* sources, uint64_t n_sources, int hop,
+                      uint64_t root_degree, int threads, uint64_t* view_row_ptrs, uint32_t* view_cols, uint64_t cols_cap, uint64_t* n_cols) {
+  const int T = nthreads(threads);
+  std::vector<uint8_t> in_view(V, 0);
+  std::vector<uint32_t> frontier;
+  frontier.reserve(n_sources);
+  for (uint64_t i = 0; i < n_sources; i++) {
+    uint32_t s = sources[i];
+    if (root_degree == 0 || row_ptrs[s + 1] - row_ptrs[s] >= root_degree) {
+      if (!in_view[s]) frontier.push_back(s);
+      in_view[s] = 1;
+    }
+  }
+  // breadth-first layers: a vertex at distance < hop from a kept source gets its row
+  for (int layer = 1; layer < hop; layer++) {
+    std::vector<std::vector<uint32_t>> next(T);
+#pragma omp parallel num_threads(T)
+    {
+      auto& mine = next[omp_get_thread_num()];
+#pragma omp for schedule(dynamic, 256)
+      for (int64_t i = 0; i < (int64_t)frontier.size(); i++) {
+        uint32_t x = frontier[i];
+        for (uint64_t j = row_ptrs[x]; j < row_ptrs[x + 1]; j++) {
+          uint32_t y = cols[j];
+          if (!__atomic_exchange_n(&in_view[y], (uint8_t)1, __ATOMIC_RELAXED)) mine.push_back(y);
+        }
+      }
+    }
+    frontier.clear();
+    for (auto& v : next) frontier.insert(frontier.end(), v.begin(), v.end());
+  }
+  uint64_t total = 0;
+  for (uint64_t v = 0; v < V; v++) {
+    view_row_ptrs[v] = total;
+    if (in_view[v]) total += row_ptrs[v + 1] - row_ptrs[v];
+  }
+  view_row_ptrs[V] = total;
+  *n_cols = total;
+  if (total > cols_cap) return false;
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
+  for (int64_t v = 0; v < (int64_t)V; v++)
+    if (in_view[v]) std::memcpy(view_cols + view_row_ptrs[v], cols + row_ptrs[v], (row_ptrs[v + 1] - row_ptrs[v]) * sizeof(uint32_t));
+  return true;
+}
+
+void random_pattern(int n_min, int n_max, double p, uint64_t seed, uint64_t* counter, int* n_out, uint8_t bits[7]) {
+  auto next = [&]() { return unit_double(seed, (*counter)++); };
+  while (true) {
+    int n = n_min + (int)(next() * (n_max - n_min + 1));
+    if (n > n_max) n = n_max;
+    std::memset(bits, 0, 7);
+    for (int i = 0; i < n; i++)
+      for (int j = i + 1; j < n; j++)
+        if (next() < p) {
+          bits[i] |= (uint8_t)(1u << j);
+          bits[j] |= (uint8_t)(1u << i);
+        }
+    uint32_t seen = 1, grow = 1;
+    while (grow) {
+      uint32_t add = 0;
+      for (int i = 0; i < n; i++)
+        if (seen >> i & 1) add |= bits[i];
+      grow = add & ~seen;
+      seen |= add;
+    }
+    if (seen == (1u << n) - 1) {
+      *n_out = n;
+      return;
+    }
+  }
+}
+
+}  // namespace vsgm

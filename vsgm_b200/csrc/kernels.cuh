@@ -1,0 +1,515 @@
+// Device kernels of the enumeration engine (sm_100a).
+//
+// Partial matches live in HBM as a "frame": SoA columns of matched data-vertex
+// ids (one u32 column per materialised pattern vertex) plus, per computed but
+// unmaterialised pattern vertex u, a candidate set per path given as
+// (begin u64, length u32) into a u32 pool (the reference keeps an index into a
+// per-parent offsets array instead, src/executor/im_data.h:7-90).  A pool may be
+// the view's own adjacency array: a candidate set that is a contiguous slice of
+// one adjacency list is never copied.
+//
+// All kernels are integer-only.  Intersections are warp-per-path: the warp
+// restricts every backward neighbour's adjacency list to the value window the
+// order conditions allow, takes the shortest restricted list as the pivot, and
+// its lanes walk the pivot while galloping forward through the other lists
+// (each lane's candidates increase, so every search resumes where the lane's
+// previous one ended).  The reference walks the whole pivot list and
+// binary-searches every other list from scratch for every element
+// (src/gpu/gpu_utils_gpsm_bin_search.h:14-130); the set produced is identical.
+#pragma once
+
+#include <cstdint>
+
+#include "vsgm_plan.h"
+
+namespace vsgm {
+namespace dev {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+struct Frame {
+  uint64_t P;                    // number of partial matches
+  uint32_t* col[VSGM_MAX_QV];    // materialised columns
+  uint64_t* cbeg[VSGM_MAX_QV];   // candidate-set begin per path
+  uint32_t* clen[VSGM_MAX_QV];   // candidate-set length per path
+  const uint32_t* pool[VSGM_MAX_QV];
+};
+
+// Everything a kernel needs about one op, small enough to pass by value.
+// Warp kernels load the path's materialised values once (lane i holds the value
+// of pattern vertex m[i]) and read them by shuffle: bs[] and cs[] are lane slots.
+struct OpDesc {
+  uint8_t u;                    // pattern vertex of the op
+  uint8_t nb;                   // backward neighbours (intersection inputs)
+  uint8_t b[VSGM_MAX_QV];
+  uint8_t bs[VSGM_MAX_QV];      // lane slot of b[j]
+  uint8_t nc;                   // conditions: candidate cop[i] value(cv[i])
+  uint8_t cop[VSGM_MAX_QV];
+  uint8_t cv[VSGM_MAX_QV];
+  uint8_t cs[VSGM_MAX_QV];      // lane slot of cv[i]
+  uint8_t nm;                   // materialised vertices whose columns are read
+  uint8_t m[VSGM_MAX_QV];
+  int8_t other;                 // COMPUTE_COUNT: computed vertex to count against (-1: none)
+  uint8_t other_op;             // relation candidate(u) OP candidate(other)
+};
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// first position in a[lo, hi) with a[pos] >= x (hi if none), probing forward from lo
+__device__ __forceinline__ uint64_t gallop(const uint32_t* __restrict__ a, uint64_t lo, uint64_t hi, uint32_t x) {
+  if (lo >= hi || __ldg(a + lo) >= x) return lo;
+  uint64_t step = 1;
+  while (lo + step < hi && __ldg(a + lo + step) < x) {
+    lo += step;
+    step <<= 1;
+  }
+  uint64_t l = lo + 1, r = (lo + step < hi) ? lo + step : hi;
+  while (l < r) {
+    uint64_t mid = (l + r) >> 1;
+    if (__ldg(a + mid) < x)
+      l = mid + 1;
+    else
+      r = mid;
+  }
+  return l;
+}
+
+__device__ __forceinline__ uint64_t lower_bound(const uint32_t* __restrict__ a, uint64_t lo, uint64_t hi, uint64_t x) {
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    if ((uint64_t)__ldg(a + mid) < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Per-path condition state: candidates must lie in [lo, hi) and differ from ne[].
+struct Window {
+  uint64_t lo, hi;
+  uint32_t ne[VSGM_MAX_QV];
+  int nne;
+};
+
+__device__ __forceinline__ void window_add(Window* w, uint8_t op, uint32_t v, int i) {
+  if (op == VSGM_LARGER_THAN) {
+    if ((uint64_t)v + 1 > w->lo) w->lo = (uint64_t)v + 1;
+  } else if (op == VSGM_LESS_THAN) {
+    if ((uint64_t)v < w->hi) w->hi = v;
+  } else if (op == VSGM_NON_EQUAL) {
+    w->ne[i] = v;  // slot i; unused slots keep a value that never matches
+  }
+}
+
+// warp version: `mine` is this lane's gathered value (see gather_lane)
+__device__ __forceinline__ void make_window(const OpDesc& d, uint32_t mine, Window* w) {
+  w->lo = 0;
+  w->hi = 0x100000000ull;
+  w->nne = d.nc;
+#pragma unroll
+  for (int i = 0; i < VSGM_MAX_QV; i++) {
+    uint32_t v = __shfl_sync(kFull, mine, d.cs[i]);
+    w->ne[i] = 0xffffffffu;
+    if (i < d.nc) window_add(w, d.cop[i], v, i);
+  }
+}
+
+// thread version: values read straight from the frame columns
+__device__ __forceinline__ void make_window_thread(const OpDesc& d, const Frame& f, uint64_t p, Window* w) {
+  w->lo = 0;
+  w->hi = 0x100000000ull;
+  w->nne = d.nc;
+#pragma unroll
+  for (int i = 0; i < VSGM_MAX_QV; i++) {
+    w->ne[i] = 0xffffffffu;
+    if (i < d.nc) window_add(w, d.cop[i], __ldg(f.col[d.cv[i]] + p), i);
+  }
+}
+
+// NON_EQUAL slots: a candidate can never equal 0xffffffff (ids are < V < 2^32 - 1)
+__device__ __forceinline__ bool ne_ok(const Window& w, uint32_t c) {
+  bool ok = true;
+#pragma unroll
+  for (int i = 0; i < VSGM_MAX_QV; i++) ok &= (c != w.ne[i]);
+  return ok;
+}
+
+// Lane i < nm loads the path's value of pattern vertex m[i].
+__device__ __forceinline__ uint32_t gather_lane(const Frame& f, const OpDesc& d, uint64_t p) {
+  const unsigned lane = lane_id();
+  return lane < d.nm ? __ldg(f.col[d.m[lane]] + p) : 0u;
+}
+
+// Restricted ranges of every backward list; pivot = shortest restricted range.
+// Lane j < nb computes list j's range; results are broadcast.
+struct Lists {
+  uint64_t s[VSGM_MAX_QV], e[VSGM_MAX_QV];
+  int pivot;
+  uint64_t ps, pe;    // the pivot's range
+  uint64_t full_min;  // least unrestricted degree (for the algorithmic-byte count)
+};
+
+__device__ __forceinline__ void restrict_lists(const OpDesc& d, uint32_t mine, const Window& w, const uint64_t* __restrict__ rp,
+                                               const uint32_t* __restrict__ ci, Lists* L) {
+  const unsigned lane = lane_id();
+  uint64_t s = 0, e = 0, deg = ~0ull;
+  const uint32_t v = __shfl_sync(kFull, mine, d.bs[lane < d.nb ? lane : 0]);
+  if (lane < d.nb) {
+    uint64_t a = __ldg(rp + v), z = __ldg(rp + v + 1);
+    deg = z - a;
+    s = (w.lo > 0) ? lower_bound(ci, a, z, w.lo) : a;
+    e = (w.hi <= 0xffffffffull) ? lower_bound(ci, s, z, w.hi) : z;
+    if (e < s) e = s;
+  }
+  uint64_t best = ~0ull;
+  int piv = 0;
+  L->full_min = ~0ull;
+#pragma unroll
+  for (int i = 0; i < VSGM_MAX_QV; i++) {
+    uint64_t si = __shfl_sync(kFull, s, i), ei = __shfl_sync(kFull, e, i), di = __shfl_sync(kFull, deg, i);
+    L->s[i] = si;
+    L->e[i] = ei;
+    if (i < d.nb) {
+      if (ei - si < best) {
+        best = ei - si;
+        piv = i;
+      }
+      if (di < L->full_min) L->full_min = di;
+    }
+  }
+  L->pivot = piv;
+  L->ps = L->pe = 0;
+#pragma unroll
+  for (int i = 0; i < VSGM_MAX_QV; i++)
+    if (i == piv) {
+      L->ps = L->s[i];
+      L->pe = L->e[i];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sizing: restricted pivot length per path (upper bound of the candidate set)
+// ---------------------------------------------------------------------------
+__global__ void k_compute_size(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t* __restrict__ ub) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint32_t mine = gather_lane(f, d, p);
+    Window w;
+    make_window(d, mine, &w);
+    Lists L;
+    restrict_lists(d, mine, w, rp, ci, &L);
+    if (lane_id() == 0) ub[p] = L.pe - L.ps;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// COMPUTE with one backward neighbour and no exclusion: the candidate set is a
+// slice of one adjacency list; record it without copying.
+// ---------------------------------------------------------------------------
+__global__ void k_compute_slice(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t* __restrict__ beg,
+                                uint32_t* __restrict__ len, unsigned long long* __restrict__ total) {
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long mine = 0;
+  for (uint64_t p = tid; p < f.P; p += nthreads) {
+    Window w;
+    make_window_thread(d, f, p, &w);
+    const uint32_t v = __ldg(f.col[d.b[0]] + p);
+    uint64_t a = __ldg(rp + v), z = __ldg(rp + v + 1);
+    uint64_t s = (w.lo > 0) ? lower_bound(ci, a, z, w.lo) : a;
+    uint64_t e = (w.hi <= 0xffffffffull) ? lower_bound(ci, s, z, w.hi) : z;
+    if (e < s) e = s;
+    beg[p] = s;
+    len[p] = (uint32_t)(e - s);
+    mine += e - s;
+  }
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
+  if (lane_id() == 0 && mine) atomicAdd(total, mine);
+}
+
+// ---------------------------------------------------------------------------
+// COMPUTE: write the sorted candidate set of every path at pool[off[p]...]
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void k_compute_write(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint64_t* __restrict__ off,
+                                uint32_t* __restrict__ pool, uint32_t* __restrict__ len) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint32_t mine = gather_lane(f, d, p);
+    Window w;
+    make_window(d, mine, &w);
+    Lists L;
+    restrict_lists(d, mine, w, rp, ci, &L);
+    const uint64_t ps = L.ps, pe = L.pe;
+    uint64_t pos[NB];
+#pragma unroll
+    for (int j = 0; j < NB; j++) pos[j] = L.s[j];
+    uint32_t* out = pool + off[p];
+    uint32_t written = 0;
+    for (uint64_t base = ps; base < pe; base += kWarp) {
+      const uint64_t k = base + lane;
+      bool ok = false;
+      uint32_t c = 0;
+      if (k < pe) {
+        c = __ldg(ci + k);
+        ok = ne_ok(w, c);
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+          if (j == L.pivot || !ok) continue;
+          uint64_t q = gallop(ci, pos[j], L.e[j], c);
+          pos[j] = q;
+          ok = (q < L.e[j]) && (__ldg(ci + q) == c);
+        }
+      }
+      unsigned mask = __ballot_sync(kFull, ok);
+      if (ok) out[written + __popc(mask & ((1u << lane) - 1))] = c;
+      written += __popc(mask);
+    }
+    if (lane == 0) len[p] = written;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// COMPUTE_COUNT: count valid candidates (or, with a computed vertex `other`,
+// the candidates of other standing in relation to each) and add to *total.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t count_vs(const uint32_t* __restrict__ a, uint64_t n, uint64_t* cur, uint32_t c, uint8_t op) {
+  // elements x of a with  c op x ; *cur is a lower bound of the search position
+  uint64_t q = gallop(a, *cur, n, c);
+  *cur = q;
+  bool eq = q < n && __ldg(a + q) == c;
+  if (op == VSGM_LESS_THAN) return n - q - (eq ? 1 : 0);
+  if (op == VSGM_LARGER_THAN) return q;
+  return n - (eq ? 1 : 0);
+}
+
+template <int NB, bool kOther, bool kBytes>
+__global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                                       unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  unsigned long long acc = 0, acc_bytes = 0;
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint32_t mine = gather_lane(f, d, p);
+    Window w;
+    make_window(d, mine, &w);
+    Lists L;
+    restrict_lists(d, mine, w, rp, ci, &L);
+    const uint64_t ps = L.ps, pe = L.pe;
+    if (kBytes && lane == 0) acc_bytes += 4ull * L.full_min + 16ull * NB + 4ull * d.nm;
+    uint64_t pos[NB];
+#pragma unroll
+    for (int j = 0; j < NB; j++) pos[j] = L.s[j];
+    const uint32_t* oset = nullptr;
+    uint64_t on = 0, ocur = 0;
+    if (kOther) {
+      oset = f.pool[d.other] + f.cbeg[d.other][p];
+      on = f.clen[d.other][p];
+    }
+    for (uint64_t base = ps; base < pe; base += kWarp) {
+      const uint64_t k = base + lane;
+      if (k < pe) {
+        uint32_t c = __ldg(ci + k);
+        bool ok = ne_ok(w, c);
+#pragma unroll
+        for (int j = 0; j < NB; j++) {
+          if (j == L.pivot || !ok) continue;
+          uint64_t q = gallop(ci, pos[j], L.e[j], c);
+          pos[j] = q;
+          ok = (q < L.e[j]) && (__ldg(ci + q) == c);
+        }
+        if (ok) acc += kOther ? count_vs(oset, on, &ocur, c, d.other_op) : 1ull;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    acc += __shfl_down_sync(kFull, acc, o);
+    if (kBytes) acc_bytes += __shfl_down_sync(kFull, acc_bytes, o);
+  }
+  if (lane == 0) {
+    if (acc) atomicAdd(total, acc);
+    if (kBytes && acc_bytes) atomicAdd(bytes, acc_bytes);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FILTER: keep the candidates of u that satisfy d's conditions (per path)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool cond_ok(const Window& w, uint32_t c) { return (uint64_t)c >= w.lo && (uint64_t)c < w.hi && ne_ok(w, c); }
+
+__global__ void k_filter(Frame f, OpDesc d, const uint64_t* __restrict__ off, uint32_t* __restrict__ pool, uint32_t* __restrict__ len) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint32_t mine = gather_lane(f, d, p);
+    Window w;
+    make_window(d, mine, &w);
+    const uint32_t* in = f.pool[d.u] + f.cbeg[d.u][p];
+    const uint32_t n = f.clen[d.u][p];
+    uint32_t* out = pool + off[p];
+    uint32_t written = 0;
+    for (uint32_t base = 0; base < n; base += kWarp) {
+      const uint32_t k = base + lane;
+      uint32_t c = 0;
+      bool ok = false;
+      if (k < n) {
+        c = __ldg(in + k);
+        ok = cond_ok(w, c);
+      }
+      unsigned mask = __ballot_sync(kFull, ok);
+      if (ok) out[written + __popc(mask & ((1u << lane) - 1))] = c;
+      written += __popc(mask);
+    }
+    if (lane == 0) len[p] = written;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MATERIALIZE: expand every path by its candidates of u (one thread per child;
+// the parent is found by binary search over the children offsets)
+// ---------------------------------------------------------------------------
+struct Expand {
+  uint8_t u;
+  uint8_t nm;                 // columns copied from the parent
+  uint8_t m[VSGM_MAX_QV];
+  uint8_t ncu;                // candidate references copied from the parent
+  uint8_t cu[VSGM_MAX_QV];
+};
+
+// children [c0, c1) of the whole frame; out's pointers are pre-shifted so that
+// child c is written at out.*[c]
+__global__ void k_expand(Frame in, Expand x, const uint64_t* __restrict__ off, uint64_t c0, uint64_t c1, Frame out) {
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t c = c0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < c1; c += nthreads) {
+    // parent = last p with off[p] <= c
+    uint64_t lo = 0, hi = in.P;
+    while (hi - lo > 1) {
+      uint64_t mid = (lo + hi) >> 1;
+      if (__ldg(off + mid) <= c)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const uint64_t p = lo, r = c - __ldg(off + p);
+#pragma unroll
+    for (int i = 0; i < VSGM_MAX_QV; i++)
+      if (i < x.nm) out.col[x.m[i]][c] = __ldg(in.col[x.m[i]] + p);
+    out.col[x.u][c] = __ldg(in.pool[x.u] + in.cbeg[x.u][p] + r);
+#pragma unroll
+    for (int i = 0; i < VSGM_MAX_QV; i++)
+      if (i < x.ncu) {
+        out.cbeg[x.cu[i]][c] = __ldg(in.cbeg[x.cu[i]] + p);
+        out.clen[x.cu[i]][c] = __ldg(in.clen[x.cu[i]] + p);
+      }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// COUNT
+// ---------------------------------------------------------------------------
+__global__ void k_count_one(Frame f, uint8_t u, unsigned long long* __restrict__ total) {
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  unsigned long long acc = 0;
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < f.P; p += nthreads) acc += f.clen[u][p];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if (lane_id() == 0 && acc) atomicAdd(total, acc);
+}
+
+// pairs (x0 in set u0, x1 in set u1) with x0 OP x1: walk the smaller set
+__global__ void k_count_two(Frame f, uint8_t u0, uint8_t u1, uint8_t op, unsigned long long* __restrict__ total) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  unsigned long long acc = 0;
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint32_t* a0 = f.pool[u0] + f.cbeg[u0][p];
+    const uint32_t* a1 = f.pool[u1] + f.cbeg[u1][p];
+    uint64_t n0 = f.clen[u0][p], n1 = f.clen[u1][p];
+    const uint32_t *walk = a0, *search = a1;
+    uint64_t nw = n0, ns = n1;
+    uint8_t rel = op;  // relation walked-element OP searched-element
+    if (n0 > n1) {
+      walk = a1;
+      search = a0;
+      nw = n1;
+      ns = n0;
+      rel = op == VSGM_LESS_THAN ? VSGM_LARGER_THAN : (op == VSGM_LARGER_THAN ? VSGM_LESS_THAN : op);
+    }
+    if (ns == 0) continue;
+    uint64_t cur = 0;
+    for (uint64_t k = lane; k < nw; k += kWarp) acc += count_vs(search, ns, &cur, __ldg(walk + k), rel);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if (lane == 0 && acc) atomicAdd(total, acc);
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan of u64 (three passes over 2048-element tiles)
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint64_t block_exclusive(uint64_t v, uint64_t* total) {
+  __shared__ uint64_t warp_sums[kScanThreads / kWarp];
+  const unsigned lane = lane_id(), wid = threadIdx.x / kWarp;
+  uint64_t x = v;
+  for (int o = 1; o < kWarp; o <<= 1) {
+    uint64_t y = __shfl_up_sync(kFull, x, o);
+    if (lane >= (unsigned)o) x += y;
+  }
+  if (lane == kWarp - 1) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    uint64_t s = (lane < kScanThreads / kWarp) ? warp_sums[lane] : 0;
+    for (int o = 1; o < kWarp; o <<= 1) {
+      uint64_t y = __shfl_up_sync(kFull, s, o);
+      if (lane >= (unsigned)o) s += y;
+    }
+    if (lane < kScanThreads / kWarp) warp_sums[lane] = s;
+  }
+  __syncthreads();
+  uint64_t before = (wid > 0 ? warp_sums[wid - 1] : 0) + x - v;
+  *total = warp_sums[kScanThreads / kWarp - 1];
+  __syncthreads();
+  return before;
+}
+
+// in may be a u64 or u32 array (kIn32)
+template <bool kIn32>
+__global__ void k_scan_tiles(const void* __restrict__ in, uint64_t n, uint64_t* __restrict__ tile_sums) {
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  uint64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++)
+    if (base + i < n) s += kIn32 ? (uint64_t)((const uint32_t*)in)[base + i] : ((const uint64_t*)in)[base + i];
+  uint64_t total;
+  block_exclusive(s, &total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+template <bool kIn32>
+__global__ void k_scan_apply(const void* __restrict__ in, uint64_t n, const uint64_t* __restrict__ tile_prefix, uint64_t* __restrict__ out) {
+  const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  uint64_t v[kScanItems];
+  uint64_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) {
+    v[i] = (base + i < n) ? (kIn32 ? (uint64_t)((const uint32_t*)in)[base + i] : ((const uint64_t*)in)[base + i]) : 0;
+    s += v[i];
+  }
+  uint64_t total;
+  uint64_t run = block_exclusive(s, &total) + tile_prefix[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) {
+    if (base + i < n) out[base + i] = run;
+    run += v[i];
+  }
+  // out[n] = grand total, written by the block that owns the last element
+  if (base < n && base + kScanItems >= n) out[n] = run;
+}
+
+}  // namespace dev
+}  // namespace vsgm
