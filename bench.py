@@ -1,0 +1,285 @@
+"""Benchmark: exact subgraph counting on one B200 (matches/s), pm_pipeline workload.
+
+Workload (N=1): synthetic R-MAT scale 22 (4.19M vertices), edge factor 16,
+a/b/c/d = 0.57/0.19/0.19/0.05, seed 2, self-loops and duplicates removed,
+symmetrised, uint32 CSR with sorted rows; queries: 4-clique (-kc 4), 4-cycle
+(-p 1) and diamond (-p 2), planned by the reference heuristic; one view holding
+every source (what view_packing produces for this graph under a 40 GB budget).
+A step is one match of all three queries over the resident view.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value   = sum of the exact counts / device time per step (inputs resident in HBM)
+e2e     = the same through the C ABI from pinned host buffers: view upload +
+          match + count read-back inside the timed region
+roofline: dominant kernel (COMPUTE_COUNT) algorithmic bytes / its device time
+cpu_baseline / --impl reference: the CPU restatement of the reference executor
+          (oracle/) on a time-boxed random sample of roots, all host cores.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = {"workload": "rmat22_ef16_seed2_kc4_p1_p2", "graph": "R-MAT scale 22, edge factor 16, a/b/c=0.57/0.19/0.19, seed 2",
+            "queries": ["-kc 4", "-p 1", "-p 2"], "views": 1}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_workload(vs, scale=22, edge_factor=16, seed=2):
+    t = time.time()
+    g = vs.gen_rmat(scale, edge_factor, 0.57, 0.19, 0.19, seed=seed)
+    plans = [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2)]
+    log(f"graph V={g.V} E={g.E} generated in {time.time() - t:.1f}s; plans:", [p.describe() for p in plans])
+    return g, plans
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, path):
+        self.path = path
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200", "-i", "0"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = sorted(float(r[1]) for r in rows)
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(n)
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_sample_rate(g, plans, seconds, threads):
+    """Time-boxed oracle run: random roots in chunks until `seconds` elapse."""
+    import oracle
+    rng = np.random.default_rng(12345)
+    roots = rng.permutation(g.V).astype(np.uint32)
+    per_plan = seconds / len(plans)
+    total_count, total_time, roots_done = 0, 0.0, 0
+    chunk = 64
+    for p in plans:
+        t_plan, i = 0.0, 0
+        while t_plan < per_plan and i < len(roots):
+            src = np.sort(roots[i:i + chunk])
+            t = time.perf_counter()
+            c = oracle.count(p, g, src, threads=threads)
+            dt = time.perf_counter() - t
+            total_count += c
+            t_plan += dt
+            i += chunk
+            roots_done += len(src)
+            chunk = min(chunk * 2, 1 << 16) if dt < 0.5 else max(chunk // 2, 1)
+        total_time += t_plan
+    return total_count / total_time, total_count, total_time, roots_done
+
+
+def run_reference(args):
+    import torch.distributed as dist  # noqa: F401  (rank handling only)
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import vsgm_b200 as vs
+    vs.capi.lib()
+    g, plans = make_workload(vs)
+    threads = os.cpu_count() or 1
+    per_step = []
+    for s in range(args.warmup + args.steps):
+        rate, cnt, secs, nroots = cpu_sample_rate(g, plans, args.ref_seconds, threads)
+        if s >= args.warmup:
+            per_step.append((rate, cnt, secs, nroots))
+    rate = float(np.mean([r[0] for r in per_step]))
+    secs = float(np.mean([r[2] for r in per_step]))
+    sample = (f"{per_step[-1][3]} random roots of {g.V} per step (time-boxed {args.ref_seconds}s, split over the 3 queries); "
+              f"matches/s = sampled matches / sampled seconds")
+    out = {"impl": "reference", "metric": "matches/s", "value": rate, "unit": "matches/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+           "dtype": "u32", "data": "synthetic", "config": WORKLOAD,
+           "cpu_baseline": {"value": rate, "unit": "matches/s", "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": rate, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--ref-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import vsgm_b200 as vs
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    g, plans = make_workload(vs, scale=args.scale)
+    # roots of this rank: a strided share of the vertices (one view per rank)
+    roots = np.arange(rank, g.V, world, dtype=np.uint32)
+    eng = vs.Engine(g.V, plans, device=local)
+    stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+
+    # ---------------- device-resident timing (value)
+    eng.transfer_view(g, roots)
+    eng.set_profiling(True)
+    for _ in range(args.warmup):
+        eng.match()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    eng.reset_counts()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    op_ms = {}
+    op_bytes = {}
+    launches = 0
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    with Clocks(os.path.join(ROOT, "gpurun_out", "bench_clocks.csv")) as ck:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            eng.match()
+            for pi, p in enumerate(plans):
+                s = eng.stats(pi)
+                for i in range(p.n_ops):
+                    key = (pi, i)
+                    op_ms[key] = op_ms.get(key, 0.0) + s.op_ms[i]
+                    op_bytes[key] = op_bytes.get(key, 0) + s.op_bytes[i]
+                    launches += s.op_launches[i]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    clocks = ck.summary()
+    step_ms = ev0.elapsed_time(ev1) / args.steps
+    counts = [c // args.steps for c in eng.counts()]
+    if world > 1:
+        t = torch.tensor([step_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        step_ms = float(t.item())
+        ct = torch.tensor(counts, dtype=torch.int64, device="cuda")
+        torch.distributed.all_reduce(ct)
+        counts = [int(x) for x in ct.tolist()]
+    matches = sum(counts)
+    value = matches / (step_ms / 1e3)
+
+    # dominant kernel: the op with the largest device time
+    (dom_plan, dom_op), dom_ms = max(op_ms.items(), key=lambda kv: kv[1])
+    dom_ms /= args.steps
+    dom_bytes = op_bytes.get((dom_plan, dom_op), 0) / args.steps
+    peak, peak_kind = load_peaks()
+    achieved = (dom_bytes / (dom_ms / 1e3)) / 1e9 if dom_ms > 0 and dom_bytes > 0 else None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "traffic": None, "kernel": f"plan {dom_plan} op {dom_op} ({vs.capi.OP_NAMES[plans[dom_plan].op_type[dom_op]]})",
+                "kernel_ms_per_step": dom_ms, "peak_kind": peak_kind}
+    per_query = []
+    for pi, p in enumerate(plans):
+        ms = sum(v for (a, _), v in op_ms.items() if a == pi) / args.steps
+        per_query.append({"query": WORKLOAD["queries"][pi], "count": counts[pi], "device_ms": ms})
+
+    # ---------------- end to end through the C ABI from pinned host buffers
+    eng.set_profiling(False)
+    h_rp = torch.from_numpy(g.row_ptrs.view(np.int64)).pin_memory()
+    h_ci = torch.from_numpy(g.cols.view(np.int32)).pin_memory()
+    h_src = torch.from_numpy(roots.view(np.int32)).pin_memory()
+    L = vs.capi.lib()
+    import ctypes as C
+    e2e_ms = []
+    for s in range(args.warmup + args.steps):
+        eng.reset_counts()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        vs.capi.check(L.vsgm_transfer_view(eng.h, C.cast(h_rp.data_ptr(), C.POINTER(C.c_uint64)), C.cast(h_ci.data_ptr(), C.POINTER(C.c_uint32)),
+                                           g.E, C.cast(h_src.data_ptr(), C.POINTER(C.c_uint32)), len(roots)), eng.h)
+        eng.match()
+        got = eng.counts()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        if s >= args.warmup:
+            e2e_ms.append(t0.elapsed_time(t1))
+    e2e_step = float(np.mean(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_step], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    e2e = {"value": matches / (e2e_step / 1e3), "unit": "matches/s", "h2d_bytes_per_step": int(8 * (g.V + 1) + 4 * g.E + 4 * len(roots)),
+           "d2h_bytes_per_step": 8 * len(plans), "ms_per_step": e2e_step}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        rate, cnt, secs, nroots = cpu_sample_rate(g, plans, args.cpu_seconds, threads)
+        cpu = {"value": rate, "unit": "matches/s", "cores": threads, "kind": "port",
+               "sample": f"{nroots} random roots (time-boxed {args.cpu_seconds}s over the 3 queries), matches/s = sampled matches / seconds"}
+
+    if rank == 0:
+        out = {"metric": "matches/s", "value": value, "unit": "matches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": step_ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
+               "data": "synthetic", "config": dict(WORKLOAD, scale=args.scale, l2="inputs larger than L2 (cols 0.5 GB)",
+                                                     parallelism=f"roots strided over {world} GPU(s)"),
+               "counts": counts, "per_query": per_query, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+               "gpu_launches": int(launches), "clocks": clocks}
+        print(json.dumps(out), flush=True)
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -88,6 +88,14 @@ int vsgm_gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t 
  * seed at *counter; advances *counter. */
 int vsgm_random_pattern(int n_min, int n_max, double p, uint64_t seed, uint64_t* counter, int* n, uint8_t* adj_bits);
 
+/* Degree-ordered relabelling of a whole graph (no reference counterpart; the
+ * reference keeps the input's ids).  new id = rank of (degree, old id), ascending
+ * when `ascending`, else descending; new_of_old[V], row_ptrs_out[V+1], cols_out[E]
+ * are caller-allocated.  Exact total counts are invariant to relabelling; apply
+ * the same permutation to a .vbmap (bins_new[new_of_old[v]] = bins[v]). */
+int vsgm_degree_relabel(uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, int ascending, int threads, uint32_t* new_of_old,
+                        uint64_t* row_ptrs_out, uint32_t* cols_out);
+
 /* ViewBin::Materialize (src/view/view_bin.h:66-142): full-V CSR holding the
  * adjacency rows of every source with degree >= root_degree (all when 0) and of
  * every vertex within hop-1 steps of one.  view_row_ptrs has V+1 entries; fails
@@ -135,6 +143,43 @@ typedef struct vsgm_plan_stats {
   uint64_t peak_bytes;                /* peak working memory */
 } vsgm_plan_stats;
 int vsgm_get_stats(vsgm_engine* e, int plan, vsgm_plan_stats* out);
+
+/* Batched execution (no reference counterpart: the reference runs one plan at a
+ * time over one view, src/executor/pipeline_executor.h:83-109).  vsgm_add_view
+ * uploads another view (its own vertex count) and keeps it resident;
+ * vsgm_run_batched runs every (plan, view) pair of the given ids in ONE
+ * persistent launch fed by a device work queue of root ranges, and writes
+ * counts[p * n_views + v] (exact uint64). */
+int vsgm_add_view(vsgm_engine* e, uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n_cols, const uint32_t* sources,
+                  uint64_t n_sources, int* view_id);
+int vsgm_run_batched(vsgm_engine* e, const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* counts);
+
+typedef struct vsgm_batch_stats {
+  uint64_t tasks;         /* root-range tasks in the last batched run */
+  uint64_t launches;      /* kernels launched by it */
+  uint64_t scratch_bytes; /* per-warp scratch allocated */
+  double ms;              /* device time (with profiling on) */
+} vsgm_batch_stats;
+int vsgm_get_batch_stats(vsgm_engine* e, vsgm_batch_stats* out);
+
+/* ------------------------------------------------------------- learned planner
+ * No reference counterpart: the reference's only order heuristic is
+ * Plan::GenerateSearchSequence (src/query/plan.h:210-265).  A 3-layer MLP
+ * (n_in -> n_hidden -> n_hidden -> n_out, ReLU) whose GEMMs take BF16 operands
+ * and accumulate in FP32, trained with Adam on FP32 master weights.  Parameters
+ * are packed W1[n_in][n_hidden], b1, W2[n_hidden][n_hidden], b2,
+ * W3[n_hidden][n_out], b3.  Host arrays are row-major float. */
+typedef struct vsgm_mlp vsgm_mlp;
+int vsgm_mlp_create(int device, int n_in, int n_hidden, int n_out, uint64_t seed, vsgm_mlp** out);
+uint64_t vsgm_mlp_num_params(vsgm_mlp* m);
+int vsgm_mlp_get_params(vsgm_mlp* m, float* host);
+int vsgm_mlp_set_params(vsgm_mlp* m, const float* host);
+int vsgm_mlp_forward(vsgm_mlp* m, const float* x, int batch, float* y);
+/* masked MSE loss and its gradient w.r.t. every parameter (packed like the params) */
+int vsgm_mlp_gradients(vsgm_mlp* m, const float* x, const float* target, const float* mask, int batch, float* loss, float* grads);
+int vsgm_mlp_train_step(vsgm_mlp* m, const float* x, const float* target, const float* mask, int batch, float lr, float* loss);
+const char* vsgm_mlp_error(vsgm_mlp* m);
+int vsgm_mlp_destroy(vsgm_mlp* m);
 
 /* Collect op_ms / op_bytes (adds CUDA events and a small accounting pass). */
 int vsgm_set_profiling(vsgm_engine* e, int on);

@@ -110,3 +110,53 @@ def test_engine_rejects_bad_views(vs, graphs):
             e.transfer_view(g, np.array([g.V + 5], dtype=np.uint32))
         with pytest.raises(vs.VsgmError):
             e.match()  # no view transferred yet
+
+
+def test_pm_pipeline_driver(vs, orc, graphs, tmp_path):
+    """The drop-in CLI reads a .bin and its .vbmap and prints the reference's lines."""
+    import re
+    import subprocess
+
+    from vsgm_b200 import build
+
+    g = graphs["rmat8"]
+    path = tmp_path / "g.bin"
+    vs.write_csr_bin(path, g)
+    bins = (np.arange(g.V) * 7 % 3).astype(np.int32)
+    vs.write_vbmap(str(path) + ".2.hop.vbmap", bins, 3)
+    for args, plan in [(["-kc", "4"], vs.plan_clique(4)), (["-p", "4"], vs.plan_pattern(4))]:
+        out = subprocess.run([build.DRIVER, "-f", str(path), "-m", "1", "-t", "2", "-qs", "2", "-pn", "2", "-cn", "1", "-ds", "1"] + args,
+                             capture_output=True, text=True, timeout=300)
+        assert out.returncode == 0, out.stderr
+        got = int(re.search(r"total count for query 0: (\d+)", out.stdout).group(1))
+        assert got == orc.count(plan, g)
+        assert re.search(r"finish total time, elapsed_time=[0-9.]+ms", out.stdout)
+
+
+def test_batched_persistent_run_matches_oracle(vs, orc, graphs):
+    """Many plans x many views in one persistent launch (vsgm_run_batched)."""
+    views = [graphs["rmat7"], graphs["rmat8"], graphs["chunglu"], complete_graph(vs, 9), cycle_graph(vs, 12)]
+    named = all_plans(vs)
+    ctr = 0
+    for _ in range(16):
+        n, bits, ctr = vs.random_pattern(seed=3, counter=ctr, n_min=3, n_max=6)
+        named.append(("rand", vs.plan_query_bits(n, bits)))
+    plans = [p for _, p in named]
+    V = max(g.V for g in views)
+    with vs.Engine(V, plans) as e:
+        ids = [e.add_view(g) for g in views]
+        got = e.run_batched(ids)
+        st = e.batch_stats()
+        assert st.launches == 1 and st.tasks >= len(plans) * len(views)
+    for pi, (name, p) in enumerate(named):
+        want = [orc.count(p, g) for g in views]
+        assert got[pi] == want, (name, p.describe())
+
+
+def test_batched_run_with_partial_sources(vs, orc, graphs):
+    g = graphs["rmat8"]
+    p = vs.plan_pattern(4)
+    src = np.arange(0, g.V, 3, dtype=np.uint32)
+    with vs.Engine(g.V, [p]) as e:
+        vid = e.add_view(g, src)
+        assert e.run_batched([vid]) == [[orc.count(p, g, src)]]

@@ -22,7 +22,7 @@ __all__ = [
     "Plan", "PlanStats", "VsgmError", "Graph", "Engine",
     "plan_pattern", "plan_clique", "plan_query", "plan_graphlets", "plan_reorder", "automorphisms",
     "gen_rmat", "gen_chung_lu", "random_pattern", "read_csr_bin", "write_csr_bin", "read_vbmap", "write_vbmap",
-    "csr_defects", "materialize_view", "sources_of_bins",
+    "csr_defects", "materialize_view", "sources_of_bins", "degree_relabel",
 ]
 
 
@@ -155,6 +155,16 @@ def csr_defects(g):
     return int(_L().vsgm_csr_defects(g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32)))
 
 
+def degree_relabel(g, ascending=True, threads=0):
+    """Relabel by (degree, id) rank; returns (relabelled graph, new_of_old)."""
+    perm = np.zeros(g.V, np.uint32)
+    rp = np.zeros(g.V + 1, np.uint64)
+    ci = np.zeros(max(g.E, 1), np.uint32)
+    capi.check(_L().vsgm_degree_relabel(g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32), 1 if ascending else 0, threads,
+                                        capi.ptr(perm, C.c_uint32), capi.ptr(rp, C.c_uint64), capi.ptr(ci, C.c_uint32)))
+    return Graph(rp, ci[:g.E]), perm
+
+
 def sources_of_bins(bins, n_bins):
     """Per-bin ascending source lists (ViewBinManager::LoadViewBinPartition, src/view/view_bin_manager.h:43-60)."""
     order = np.argsort(bins, kind="stable").astype(np.uint32)
@@ -215,6 +225,28 @@ class Engine:
     def stats(self, plan=0):
         s = PlanStats()
         capi.check(_L().vsgm_get_stats(self.h, plan, C.byref(s)), self.h)
+        return s
+
+    def add_view(self, view, sources=None):
+        """Upload another view and keep it resident for run_batched; returns its id."""
+        src = np.arange(view.V, dtype=np.uint32) if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+        vid = C.c_int()
+        capi.check(_L().vsgm_add_view(self.h, view.V, capi.ptr(view.row_ptrs, C.c_uint64), capi.ptr(view.cols, C.c_uint32), view.E,
+                                      capi.ptr(src, C.c_uint32), len(src), C.byref(vid)), self.h)
+        return vid.value
+
+    def run_batched(self, view_ids, plan_ids=None):
+        """Every (plan, view) pair in one persistent launch; returns counts[plan][view]."""
+        plan_ids = list(range(len(self.plans))) if plan_ids is None else list(plan_ids)
+        v = (C.c_int * len(view_ids))(*view_ids)
+        p = (C.c_int * len(plan_ids))(*plan_ids)
+        out = np.zeros(len(plan_ids) * len(view_ids), np.uint64)
+        capi.check(_L().vsgm_run_batched(self.h, v, len(view_ids), p, len(plan_ids), capi.ptr(out, C.c_uint64)), self.h)
+        return [[int(x) for x in out[i * len(view_ids):(i + 1) * len(view_ids)]] for i in range(len(plan_ids))]
+
+    def batch_stats(self):
+        s = capi.BatchStats()
+        capi.check(_L().vsgm_get_batch_stats(self.h, C.byref(s)), self.h)
         return s
 
     def set_profiling(self, on=True):

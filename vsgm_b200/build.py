@@ -22,7 +22,7 @@ DRIVER = os.path.join(PKG, "pm_pipeline")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SRCS = ["planner.cpp", "graph.cpp", "capi_host.cpp"]
-CUDA_SRCS = ["engine.cu"]
+CUDA_SRCS = ["engine.cu", "mlp.cu"]
 
 
 def _newest(paths):

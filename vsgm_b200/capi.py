@@ -84,6 +84,10 @@ class Plan(C.Structure):
         }
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("tasks", C.c_uint64), ("launches", C.c_uint64), ("scratch_bytes", C.c_uint64), ("ms", C.c_double)]
+
+
 class PlanStats(C.Structure):
     _fields_ = [
         ("op_paths", C.c_uint64 * MAX_OPS),
@@ -120,6 +124,7 @@ _SIGS = {
                                 _u64p, _u64p, _P(_u64p), _P(_u32p)]),
     "vsgm_gen_chung_lu": (C.c_int, [C.c_uint64, C.c_uint64, C.c_double, C.c_uint64, C.c_uint64, C.c_int,
                                     _u64p, _P(_u64p), _P(_u32p)]),
+    "vsgm_degree_relabel": (C.c_int, [C.c_uint64, _u64p, _u32p, C.c_int, C.c_int, _u32p, _u64p, _u32p]),
     "vsgm_random_pattern": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_uint64, _u64p, _P(C.c_int), _u8p]),
     "vsgm_view_materialize": (C.c_int, [C.c_uint64, _u64p, _u32p, _u32p, C.c_uint64, C.c_int, C.c_uint64, C.c_int,
                                         _u64p, _u32p, C.c_uint64, _u64p]),
@@ -131,9 +136,21 @@ _SIGS = {
     "vsgm_reset_counts": (C.c_int, [C.c_void_p]),
     "vsgm_get_stats": (C.c_int, [C.c_void_p, C.c_int, _P(PlanStats)]),
     "vsgm_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "vsgm_add_view": (C.c_int, [C.c_void_p, C.c_uint64, _u64p, _u32p, C.c_uint64, _u32p, C.c_uint64, _P(C.c_int)]),
+    "vsgm_run_batched": (C.c_int, [C.c_void_p, _P(C.c_int), C.c_int, _P(C.c_int), C.c_int, _u64p]),
+    "vsgm_get_batch_stats": (C.c_int, [C.c_void_p, _P(BatchStats)]),
     "vsgm_engine_stream": (C.c_void_p, [C.c_void_p]),
     "vsgm_engine_error": (C.c_char_p, [C.c_void_p]),
     "vsgm_destroy": (C.c_int, [C.c_void_p]),
+    "vsgm_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, _P(C.c_void_p)]),
+    "vsgm_mlp_num_params": (C.c_uint64, [C.c_void_p]),
+    "vsgm_mlp_get_params": (C.c_int, [C.c_void_p, _P(C.c_float)]),
+    "vsgm_mlp_set_params": (C.c_int, [C.c_void_p, _P(C.c_float)]),
+    "vsgm_mlp_forward": (C.c_int, [C.c_void_p, _P(C.c_float), C.c_int, _P(C.c_float)]),
+    "vsgm_mlp_gradients": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_int, _P(C.c_float), _P(C.c_float)]),
+    "vsgm_mlp_train_step": (C.c_int, [C.c_void_p, _P(C.c_float), _P(C.c_float), _P(C.c_float), C.c_int, C.c_float, _P(C.c_float)]),
+    "vsgm_mlp_error": (C.c_char_p, [C.c_void_p]),
+    "vsgm_mlp_destroy": (C.c_int, [C.c_void_p]),
 }
 
 EXPORTED = sorted(_SIGS)

@@ -166,6 +166,21 @@ int vsgm_gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t 
   return VSGM_OK;
 }
 
+int vsgm_degree_relabel(uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, int ascending, int threads, uint32_t* new_of_old,
+                        uint64_t* row_ptrs_out, uint32_t* cols_out) {
+  if (!row_ptrs || (row_ptrs[V] && !cols) || !new_of_old || !row_ptrs_out || (row_ptrs[V] && !cols_out)) return fail(VSGM_EINVAL, "null argument");
+  vsgm::Csr g, h;
+  g.V = V;
+  g.row_ptrs.assign(row_ptrs, row_ptrs + V + 1);
+  g.cols.assign(cols, cols + row_ptrs[V]);
+  std::vector<uint32_t> perm;
+  vsgm::degree_relabel(g, ascending != 0, threads, &perm, &h);
+  std::memcpy(new_of_old, perm.data(), V * sizeof(uint32_t));
+  std::memcpy(row_ptrs_out, h.row_ptrs.data(), (V + 1) * sizeof(uint64_t));
+  if (h.cols.size()) std::memcpy(cols_out, h.cols.data(), h.cols.size() * sizeof(uint32_t));
+  return VSGM_OK;
+}
+
 int vsgm_random_pattern(int n_min, int n_max, double p, uint64_t seed, uint64_t* counter, int* n, uint8_t* adj_bits) {
   if (n_min < 2 || n_max > VSGM_MAX_QV || n_min > n_max || p <= 0 || !counter || !n || !adj_bits) return fail(VSGM_EINVAL, "bad pattern parameters");
   vsgm::random_pattern(n_min, n_max, p, seed, counter, n, adj_bits);

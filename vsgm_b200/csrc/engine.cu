@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "dfs.cuh"
 #include "kernels.cuh"
 #include "vsgm.h"
 
@@ -103,6 +104,17 @@ struct vsgm_engine {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
 
+  // resident views for batched runs (vsgm_add_view)
+  struct ResidentView {
+    uint64_t V = 0, n_cols = 0, n_src = 0, max_deg = 0;
+    uint64_t* rp = nullptr;
+    uint32_t* ci = nullptr;
+    uint32_t* src = nullptr;
+    std::vector<uint64_t> h_deg_src;  // degree of each source (task costing)
+  };
+  std::vector<ResidentView> rviews;
+  vsgm_batch_stats bstats{};
+
   // per-match state
   const vsgm_plan* plan = nullptr;
   vsgm_plan_stats* st = nullptr;
@@ -175,10 +187,12 @@ struct vsgm_engine {
   // like the reference's available / remaining-levels rule
   // (src/executor/processor.h:68-75)
   uint64_t level_budget(int i) const {
-    const uint64_t reserve = 1 << 20;
-    uint64_t avail = arena.avail() > reserve ? arena.avail() - reserve : 0;
-    int remaining = (int)plan->n_ops - i;
-    return avail / (uint64_t)std::max(2, remaining);
+    const uint64_t reserve = std::min<uint64_t>(1 << 20, arena.cap / 64);
+    const uint64_t avail = arena.avail() > reserve ? arena.avail() - reserve : 0;
+    const int remaining = (int)plan->n_ops - i;
+    const uint64_t share = avail / (uint64_t)std::max(2, remaining);
+    // small arenas: keep making progress with at least 64 KB while it exists
+    return std::max(share, std::min<uint64_t>(avail / 2, 1 << 16));
   }
 
   void begin_op() {
@@ -237,7 +251,7 @@ struct vsgm_engine {
       case VSGM_COMPUTE_COUNT: op_compute_count(i, f); break;
       case VSGM_COUNT: op_count(i, f); break;
       case VSGM_COMPUTE: op_compute(i, f, u); break;
-      case VSGM_FILTER_COMPUTE: op_filter(i, f, u, p.filter_cond[u], true); break;
+      case VSGM_FILTER_COMPUTE: op_filter(i, f, u); break;
       case VSGM_MATERIALIZE: op_materialize(i, f, u); break;
       default: throw OutOfMemory{"execution sequence holds an op this engine does not run"};
     }
@@ -248,7 +262,7 @@ struct vsgm_engine {
     g.P = b - a;
     for (int k = 0; k < VSGM_MAX_QV; k++) {
       if (g.col[k]) g.col[k] += a;
-      if (g.cbeg[k]) g.cbeg[k] += a;
+      if (g.cset[k]) g.cset[k] += a;
       if (g.clen[k]) g.clen[k] += a;
     }
     return g;
@@ -311,40 +325,63 @@ struct vsgm_engine {
   }
 
   template <int NB>
-  void launch_write_nb(const OpDesc& d, const Frame& f, const uint64_t* off, uint32_t* pool, uint32_t* len) {
-    k_compute_write<NB><<<grid_warps(f.P), 256, 0, stream>>>(f, d, d_rp, d_ci, off, pool, len);
+  void launch_write_nb(const OpDesc& d, const Frame& f, const uint64_t* off, uint32_t* pool, uint64_t* set, uint32_t* len) {
+    k_compute_write<NB><<<grid_warps(f.P), 256, 0, stream>>>(f, d, d_rp, d_ci, off, pool, set, len);
+  }
+
+  // Apply conditions to one sorted set per path (the adjacency list of the single
+  // backward neighbour, or the frame's candidates of u), copying only the sets
+  // that contain a NON_EQUAL value; then hand the narrowed frame to `next`.
+  template <typename Next>
+  void narrow_then(int i, const Frame& f, const OpDesc& d, bool from_adj, int u, Next&& next) {
+    const uint64_t per = 8 + 4 + 8;  // set address, length, copy bound / offset
+    uint64_t a = 0, cap_paths = ~0ull;
+    while (a < f.P) {
+      uint64_t room = std::min(cap_paths, level_budget(i) / (per + 4));
+      if (room == 0) throw OutOfMemory{"HBM budget exhausted (narrow)"};
+      uint64_t b = std::min(f.P, a + room);
+      Mark m(arena);
+      Frame g = slice(f, a, b);
+      uint64_t* set = arena.take_n<uint64_t>(g.P, "candidate sets");
+      uint32_t* len = arena.take_n<uint32_t>(g.P, "candidate lengths");
+      uint64_t* off = arena.take_n<uint64_t>(g.P + 1, "copy offsets");
+      begin_op();
+      CK(cudaMemsetAsync(d_bytes + 1, 0, sizeof(unsigned long long), stream));
+      if (from_adj)
+        k_narrow<true><<<grid_threads(g.P), 256, 0, stream>>>(g, d, d_rp, d_ci, set, len, off, d_bytes + 1);
+      else
+        k_narrow<false><<<grid_threads(g.P), 256, 0, stream>>>(g, d, d_rp, d_ci, set, len, off, d_bytes + 1);
+      CK(cudaGetLastError());
+      scan(off, false, g.P, off);
+      end_op(i, 3);
+      st->op_outputs[i] += read_u64((const uint64_t*)(d_bytes + 1));
+      const uint64_t copy = read_u64(off + g.P);
+      if (copy && 4 * copy + 4096 > arena.avail() && g.P > 1) {
+        // the copies of this slice do not fit: retry with half the paths
+        st->op_outputs[i] -= read_u64((const uint64_t*)(d_bytes + 1));
+        cap_paths = std::max<uint64_t>(1, g.P / 2);
+        continue;
+      }
+      if (copy) {
+        uint32_t* pool = arena.take_n<uint32_t>(copy, "copied candidates");
+        begin_op();
+        k_copy_marked<<<grid_warps(g.P), 256, 0, stream>>>(g, d, off, pool, set, len);
+        CK(cudaGetLastError());
+        end_op(i, 1);
+      }
+      g.cset[u] = set;
+      g.clen[u] = len;
+      st->batches++;
+      next(g);
+      a = b;
+    }
   }
 
   void op_compute(int i, const Frame& f, int u) {
     const vsgm_plan& p = *plan;
     OpDesc d = make_desc(i, p.compute_cond[u]);
-    bool has_ne = false;
-    for (int k = 0; k < d.nc; k++) has_ne |= (d.cop[k] == VSGM_NON_EQUAL);
-    if (d.nb == 1 && !has_ne) {
-      // the candidate set is a slice of one adjacency list
-      const uint64_t per = sizeof(uint64_t) + sizeof(uint32_t);
-      uint64_t a = 0;
-      while (a < f.P) {
-        uint64_t room = level_budget(i) / per;
-        if (room == 0) throw OutOfMemory{"HBM budget exhausted (COMPUTE slice)"};
-        uint64_t b = std::min(f.P, a + room);
-        Mark m(arena);
-        Frame g = slice(f, a, b);
-        uint64_t* beg = arena.take_n<uint64_t>(g.P, "candidate begins");
-        uint32_t* len = arena.take_n<uint32_t>(g.P, "candidate lengths");
-        begin_op();
-        CK(cudaMemsetAsync(d_bytes + 1, 0, sizeof(unsigned long long), stream));
-        k_compute_slice<<<grid_threads(g.P), 256, 0, stream>>>(g, d, d_rp, d_ci, beg, len, d_bytes + 1);
-        CK(cudaGetLastError());
-        end_op(i, 1);
-        st->op_outputs[i] += read_u64((const uint64_t*)(d_bytes + 1));
-        g.cbeg[u] = beg;
-        g.clen[u] = len;
-        g.pool[u] = d_ci;
-        st->batches++;
-        process(i + 1, g);
-        a = b;
-      }
+    if (d.nb == 1) {
+      narrow_then(i, f, d, true, u, [&](const Frame& g) { process(i + 1, g); });
       return;
     }
     // general case: size, scan, write
@@ -354,79 +391,51 @@ struct vsgm_engine {
     k_compute_size<<<grid_warps(f.P), 256, 0, stream>>>(f, d, d_rp, d_ci, off);
     CK(cudaGetLastError());
     scan(off, false, f.P, off);
-    end_op(i, 2);
+    end_op(i, 3);
     uint64_t a = 0;
     while (a < f.P) {
-      // each path needs 4 bytes of length plus 4 per candidate
-      uint64_t b = split_point(off, a, f.P, 4, 4 + 256, level_budget(i));
+      // each path needs a set address, a length and 4 bytes per candidate
+      uint64_t b = split_point(off, a, f.P, 4, 12, level_budget(i));
       Mark mb(arena);
       Frame g = slice(f, a, b);
       uint64_t lo = read_u64(off + a), hi = read_u64(off + b);
       uint32_t* pool = arena.take_n<uint32_t>(hi - lo, "candidate pool");
+      uint64_t* set = arena.take_n<uint64_t>(g.P, "candidate sets");
       uint32_t* len = arena.take_n<uint32_t>(g.P, "candidate lengths");
-      uint32_t* pool_eff = pool - lo;  // so that pool_eff + off[p] lies inside pool
+      uint32_t* pool_eff = pool - lo;  // pool_eff + off[p] lies inside pool
       begin_op();
       switch (d.nb) {
-        case 1: launch_write_nb<1>(d, g, off + a, pool_eff, len); break;
-        case 2: launch_write_nb<2>(d, g, off + a, pool_eff, len); break;
-        case 3: launch_write_nb<3>(d, g, off + a, pool_eff, len); break;
-        case 4: launch_write_nb<4>(d, g, off + a, pool_eff, len); break;
-        case 5: launch_write_nb<5>(d, g, off + a, pool_eff, len); break;
-        case 6: launch_write_nb<6>(d, g, off + a, pool_eff, len); break;
+        case 2: launch_write_nb<2>(d, g, off + a, pool_eff, set, len); break;
+        case 3: launch_write_nb<3>(d, g, off + a, pool_eff, set, len); break;
+        case 4: launch_write_nb<4>(d, g, off + a, pool_eff, set, len); break;
+        case 5: launch_write_nb<5>(d, g, off + a, pool_eff, set, len); break;
+        case 6: launch_write_nb<6>(d, g, off + a, pool_eff, set, len); break;
         default: throw OutOfMemory{"pattern vertex with no backward neighbour"};
       }
       CK(cudaGetLastError());
       end_op(i, 1);
       st->op_outputs[i] += hi - lo;
-      g.cbeg[u] = off + a;
+      g.cset[u] = set;
       g.clen[u] = len;
-      g.pool[u] = pool_eff;
       st->batches++;
       process(i + 1, g);
       a = b;
     }
   }
 
-  // keep the candidates of u that satisfy conds; then continue with op i+1
-  // (FILTER_COMPUTE), or return the filtered frame to the caller (MATERIALIZE)
-  void op_filter(int i, const Frame& f, int u, const vsgm_conds& conds, bool continue_next) {
-    OpDesc d = make_desc(i, conds);
+  // FILTER_COMPUTE keeps the candidates of u that satisfy the filter conditions
+  void op_filter(int i, const Frame& f, int u) {
+    OpDesc d = make_desc(i, plan->filter_cond[u]);
     d.u = (uint8_t)u;
-    Mark m(arena);
-    uint64_t* off = arena.take_n<uint64_t>(f.P + 1, "filter offsets");
-    begin_op();
-    scan(f.clen[u], true, f.P, off);
-    end_op(i, 2);
-    uint64_t a = 0;
-    while (a < f.P) {
-      uint64_t b = split_point(off, a, f.P, 4, 4 + 256, level_budget(i));
-      Mark mb(arena);
-      Frame g = slice(f, a, b);
-      uint64_t lo = read_u64(off + a), hi = read_u64(off + b);
-      uint32_t* pool = arena.take_n<uint32_t>(hi - lo, "filtered pool");
-      uint32_t* len = arena.take_n<uint32_t>(g.P, "filtered lengths");
-      uint32_t* pool_eff = pool - lo;
-      begin_op();
-      k_filter<<<grid_warps(g.P), 256, 0, stream>>>(g, d, off + a, pool_eff, len);
-      CK(cudaGetLastError());
-      end_op(i, 1);
-      g.cbeg[u] = off + a;
-      g.clen[u] = len;
-      g.pool[u] = pool_eff;
-      st->batches++;
-      if (continue_next) {
-        process(i + 1, g);
-      } else {
-        materialize_frame(i, g, u);
-      }
-      a = b;
-    }
+    narrow_then(i, f, d, false, u, [&](const Frame& g) { process(i + 1, g); });
   }
 
   void op_materialize(int i, const Frame& f, int u) {
     const vsgm_plan& p = *plan;
     if (p.materialize_cond[u].count > 0) {
-      op_filter(i, f, u, p.materialize_cond[u], false);
+      OpDesc d = make_desc(i, p.materialize_cond[u]);
+      d.u = (uint8_t)u;
+      narrow_then(i, f, d, false, u, [&](const Frame& g) { materialize_frame(i, g, u); });
     } else {
       materialize_frame(i, f, u);
     }
@@ -459,19 +468,17 @@ struct vsgm_engine {
       Frame g;
       std::memset(&g, 0, sizeof(g));
       g.P = n;
-      for (int k = 0; k < VSGM_MAX_QV; k++) g.pool[k] = f.pool[k];
       for (int k = 0; k < x.nm; k++) g.col[x.m[k]] = arena.take_n<uint32_t>(n, "child column");
       g.col[u] = arena.take_n<uint32_t>(n, "child column");
       for (int k = 0; k < x.ncu; k++) {
-        g.cbeg[x.cu[k]] = arena.take_n<uint64_t>(n, "child candidate begins");
+        g.cset[x.cu[k]] = arena.take_n<uint64_t>(n, "child candidate sets");
         g.clen[x.cu[k]] = arena.take_n<uint32_t>(n, "child candidate lengths");
       }
-      g.pool[u] = nullptr;
       // k_expand writes children [c0, c0+n) at positions [0, n): shift the outputs
       Frame shifted = g;
       for (int k = 0; k < VSGM_MAX_QV; k++) {
         if (shifted.col[k]) shifted.col[k] -= c0;
-        if (shifted.cbeg[k]) shifted.cbeg[k] -= c0;
+        if (shifted.cset[k]) shifted.cset[k] -= c0;
         if (shifted.clen[k]) shifted.clen[k] -= c0;
       }
       begin_op();
@@ -486,6 +493,124 @@ struct vsgm_engine {
   void launch_expand(const Frame& in, const Expand& x, const uint64_t* off, uint64_t c0, uint64_t n, const Frame& out) {
     k_expand<<<grid_threads(n), 256, 0, stream>>>(in, x, off, c0, c0 + n, out);
     CK(cudaGetLastError());
+  }
+
+  static DfsPlan to_dfs(const vsgm_plan& p) {
+    DfsPlan d;
+    std::memset(&d, 0, sizeof(d));
+    d.n_ops = p.n_ops;
+    d.root = p.op_vertex[0];
+    for (uint32_t i = 0; i < p.n_ops; i++) {
+      DfsOp& o = d.op[i];
+      o.type = p.op_type[i];
+      o.u = p.op_vertex[i];
+      o.other = -1;
+      const vsgm_conds* c = nullptr;
+      if (o.type == VSGM_COMPUTE || o.type == VSGM_COMPUTE_COUNT) c = &p.compute_cond[o.u];
+      if (o.type == VSGM_MATERIALIZE && i > 0) c = &p.materialize_cond[o.u];
+      if (o.type == VSGM_FILTER_COMPUTE) c = &p.filter_cond[o.u];
+      if (c) {
+        o.nc = c->count;
+        for (int k = 0; k < c->count; k++) {
+          o.cop[k] = c->op[k];
+          o.cv[k] = c->v[k];
+        }
+      }
+      if (o.type == VSGM_COMPUTE || o.type == VSGM_COMPUTE_COUNT) {
+        o.nb = p.backward[o.u].count;
+        for (int k = 0; k < o.nb; k++) o.b[k] = p.backward[o.u].v[k];
+      }
+      const vsgm_vgroup& cu = p.computed_unmat[i];
+      if (o.type == VSGM_COMPUTE_COUNT && cu.count == 1) {
+        o.other = (int8_t)cu.v[0];
+        o.other_op = p.order[o.u][cu.v[0]];
+      }
+      if (o.type == VSGM_COUNT) {
+        o.ncu = cu.count;
+        o.cu0 = cu.v[0];
+        o.cu1 = cu.count > 1 ? cu.v[1] : 0;
+        o.cu_op = cu.count > 1 ? p.order[cu.v[0]][cu.v[1]] : 0;
+      }
+    }
+    return d;
+  }
+
+  // One persistent launch over every (plan, view) pair: tasks are root ranges of
+  // balanced estimated cost, longest first, popped by warps from a device queue.
+  void run_batched(const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* out) {
+    std::vector<DfsPlan> hp(n_plans);
+    uint32_t levels = 1;
+    for (int k = 0; k < n_plans; k++) {
+      hp[k] = to_dfs(plans[plan_ids[k]]);
+      levels = std::max(levels, hp[k].n_ops);
+    }
+    std::vector<DfsView> hv(n_views);
+    uint64_t cap = 1;
+    for (int k = 0; k < n_views; k++) {
+      const ResidentView& r = rviews[view_ids[k]];
+      hv[k] = DfsView{r.rp, r.ci, r.src};
+      cap = std::max(cap, r.max_deg);
+    }
+    // task costs: sum over roots of deg^2 (wedges through the root), per plan
+    const uint64_t warps = (uint64_t)sms * 2 * kDfsWarps;  // two resident blocks per SM
+    std::vector<std::pair<double, DfsTask>> tasks;
+    double total = 0;
+    std::vector<double> work(n_views, 0);
+    for (int k = 0; k < n_views; k++) {
+      for (uint64_t d : rviews[view_ids[k]].h_deg_src) work[k] += (double)d * (double)d + 1.0;
+      total += work[k] * n_plans;
+    }
+    const double target = std::max(1.0, total / (double)(warps * 16));
+    for (int pk = 0; pk < n_plans; pk++)
+      for (int k = 0; k < n_views; k++) {
+        const auto& deg = rviews[view_ids[k]].h_deg_src;
+        uint64_t r0 = 0;
+        double acc = 0;
+        for (uint64_t r = 0; r < deg.size(); r++) {
+          acc += (double)deg[r] * (double)deg[r] + 1.0;
+          if (acc >= target || r + 1 == deg.size()) {
+            tasks.push_back({acc, DfsTask{(uint32_t)pk, (uint32_t)k, r0, r + 1}});
+            r0 = r + 1;
+            acc = 0;
+          }
+        }
+      }
+    std::stable_sort(tasks.begin(), tasks.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<DfsTask> ht(tasks.size());
+    for (size_t k = 0; k < tasks.size(); k++) ht[k] = tasks[k].second;
+
+    Mark m(arena);
+    DfsPlan* d_plans = arena.take_n<DfsPlan>(n_plans, "batched plans");
+    DfsView* d_views = arena.take_n<DfsView>(n_views, "batched views");
+    DfsTask* d_tasks = arena.take_n<DfsTask>(std::max<size_t>(1, ht.size()), "batched tasks");
+    unsigned long long* d_cnt = arena.take_n<unsigned long long>((uint64_t)n_plans * n_views + 2, "batched counts");
+    const uint64_t grid = (uint64_t)sms * 2;
+    uint32_t* scratch = arena.take_n<uint32_t>(grid * kDfsWarps * levels * cap, "per-warp scratch");
+    CK(cudaMemcpyAsync(d_plans, hp.data(), sizeof(DfsPlan) * n_plans, cudaMemcpyHostToDevice, stream));
+    CK(cudaMemcpyAsync(d_views, hv.data(), sizeof(DfsView) * n_views, cudaMemcpyHostToDevice, stream));
+    if (!ht.empty()) CK(cudaMemcpyAsync(d_tasks, ht.data(), sizeof(DfsTask) * ht.size(), cudaMemcpyHostToDevice, stream));
+    CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * ((uint64_t)n_plans * n_views + 2), stream));
+    unsigned long long* d_head = d_cnt + (uint64_t)n_plans * n_views;
+    unsigned int* d_status = (unsigned int*)(d_head + 1);
+    if (profiling) CK(cudaEventRecord(ev0, stream));
+    k_dfs<<<(unsigned)grid, kDfsWarps * kWarp, 0, stream>>>(d_plans, d_views, d_tasks, ht.size(), d_head, scratch, cap, levels, (uint32_t)n_views, d_cnt,
+                                                             d_status);
+    CK(cudaGetLastError());
+    if (profiling) CK(cudaEventRecord(ev1, stream));
+    std::vector<uint64_t> hc((uint64_t)n_plans * n_views + 2);
+    CK(cudaMemcpyAsync(hc.data(), d_cnt, sizeof(uint64_t) * hc.size(), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if ((uint32_t)hc[(uint64_t)n_plans * n_views + 1] != 0) throw OutOfMemory{"batched run: a candidate set exceeded the per-warp scratch"};
+    bstats.tasks = ht.size();
+    bstats.launches = 1;
+    bstats.scratch_bytes = grid * kDfsWarps * levels * cap * 4;
+    bstats.ms = 0;
+    if (profiling) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev0, ev1));
+      bstats.ms = ms;
+    }
+    for (uint64_t k = 0; k < (uint64_t)n_plans * n_views; k++) out[k] = hc[k];
   }
 
   void run_plan(int pi) {
@@ -680,6 +805,52 @@ void* vsgm_engine_stream(vsgm_engine* e) { return e ? (void*)e->stream : nullptr
 
 const char* vsgm_engine_error(vsgm_engine* e) { return e ? e->err.c_str() : g_engine_err.c_str(); }
 
+int vsgm_add_view(vsgm_engine* e, uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n_cols, const uint32_t* sources,
+                  uint64_t n_sources, int* view_id) {
+  if (!e || !row_ptrs || (n_cols && !cols) || (n_sources && !sources) || !view_id) return engine_fail(e, VSGM_EINVAL, "null view argument");
+  if (V == 0 || V >= 0xffffffffull || row_ptrs[V] != n_cols) return engine_fail(e, VSGM_EINVAL, "row_ptrs[V] != n_cols");
+  for (uint64_t i = 0; i < n_sources; i++)
+    if (sources[i] >= V) return engine_fail(e, VSGM_EINVAL, "source id out of range");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    vsgm_engine::ResidentView r;
+    r.V = V;
+    r.n_cols = n_cols;
+    r.n_src = n_sources;
+    for (uint64_t v = 0; v < V; v++) r.max_deg = std::max<uint64_t>(r.max_deg, row_ptrs[v + 1] - row_ptrs[v]);
+    r.h_deg_src.resize(n_sources);
+    for (uint64_t i = 0; i < n_sources; i++) r.h_deg_src[i] = row_ptrs[sources[i] + 1] - row_ptrs[sources[i]];
+    CK(cudaMalloc(&r.rp, sizeof(uint64_t) * (V + 1)));
+    CK(cudaMalloc(&r.ci, sizeof(uint32_t) * std::max<uint64_t>(1, n_cols)));
+    CK(cudaMalloc(&r.src, sizeof(uint32_t) * std::max<uint64_t>(1, n_sources)));
+    CK(cudaMemcpyAsync(r.rp, row_ptrs, sizeof(uint64_t) * (V + 1), cudaMemcpyHostToDevice, e->stream));
+    if (n_cols) CK(cudaMemcpyAsync(r.ci, cols, sizeof(uint32_t) * n_cols, cudaMemcpyHostToDevice, e->stream));
+    if (n_sources) CK(cudaMemcpyAsync(r.src, sources, sizeof(uint32_t) * n_sources, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    e->rviews.push_back(std::move(r));
+    *view_id = (int)e->rviews.size() - 1;
+  });
+}
+
+int vsgm_run_batched(vsgm_engine* e, const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* counts) {
+  if (!e || !view_ids || !plan_ids || !counts || n_views < 1 || n_plans < 1) return engine_fail(e, VSGM_EINVAL, "bad batched request");
+  for (int k = 0; k < n_views; k++)
+    if (view_ids[k] < 0 || view_ids[k] >= (int)e->rviews.size()) return engine_fail(e, VSGM_EINVAL, "unknown view id");
+  for (int k = 0; k < n_plans; k++)
+    if (plan_ids[k] < 0 || plan_ids[k] >= (int)e->plans.size()) return engine_fail(e, VSGM_EINVAL, "unknown plan id");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    e->arena.top = 0;
+    e->run_batched(view_ids, n_views, plan_ids, n_plans, counts);
+  });
+}
+
+int vsgm_get_batch_stats(vsgm_engine* e, vsgm_batch_stats* out) {
+  if (!e || !out) return engine_fail(e, VSGM_EINVAL, "null argument");
+  *out = e->bstats;
+  return VSGM_OK;
+}
+
 int vsgm_destroy(vsgm_engine* e) {
   if (!e) return VSGM_OK;
   cudaSetDevice(e->device);
@@ -689,6 +860,11 @@ int vsgm_destroy(vsgm_engine* e) {
   cudaFree(e->own_rp);
   cudaFree(e->own_ci);
   cudaFree(e->own_src);
+  for (auto& r : e->rviews) {
+    cudaFree(r.rp);
+    cudaFree(r.ci);
+    cudaFree(r.src);
+  }
   if (e->h_pinned) cudaFreeHost(e->h_pinned);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);

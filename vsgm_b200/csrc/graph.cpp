@@ -270,6 +270,34 @@ bool materialize_view(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t V
   return true;
 }
 
+void degree_relabel(const Csr& g, bool ascending, int threads, std::vector<uint32_t>* new_of_old, Csr* out) {
+  const int T = nthreads(threads);
+  const uint64_t V = g.V;
+  std::vector<uint32_t> order(V);
+  for (uint64_t v = 0; v < V; v++) order[v] = (uint32_t)v;
+  auto deg = [&](uint32_t v) { return g.row_ptrs[v + 1] - g.row_ptrs[v]; };
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+    uint64_t da = deg(a), db = deg(b);
+    if (da != db) return ascending ? da < db : da > db;
+    return a < b;
+  });
+  new_of_old->assign(V, 0);
+  for (uint64_t r = 0; r < V; r++) (*new_of_old)[order[r]] = (uint32_t)r;
+  out->V = V;
+  out->row_ptrs.assign(V + 1, 0);
+  for (uint64_t r = 0; r < V; r++) out->row_ptrs[r + 1] = out->row_ptrs[r] + deg(order[r]);
+  out->cols.resize(g.cols.size());
+  const std::vector<uint32_t>& nmap = *new_of_old;
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
+  for (int64_t r = 0; r < (int64_t)V; r++) {
+    const uint32_t v = order[r];
+    uint32_t* dst = out->cols.data() + out->row_ptrs[r];
+    uint64_t n = 0;
+    for (uint64_t j = g.row_ptrs[v]; j < g.row_ptrs[v + 1]; j++) dst[n++] = nmap[g.cols[j]];
+    std::sort(dst, dst + n);
+  }
+}
+
 void random_pattern(int n_min, int n_max, double p, uint64_t seed, uint64_t* counter, int* n_out, uint8_t bits[7]) {
   auto next = [&]() { return unit_double(seed, (*counter)++); };
   while (true) {

@@ -55,6 +55,14 @@ uint64_t csr_defects(const Csr& g);
 bool materialize_view(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t V, const uint32_t* sources, uint64_t n_sources, int hop,
                       uint64_t root_degree, int threads, uint64_t* view_row_ptrs, uint32_t* view_cols, uint64_t cols_cap, uint64_t* n_cols);
 
+// Degree-ordered relabelling: new id = rank of (degree, old id), ascending or
+// descending; rows are rewritten through the permutation and re-sorted.  Exact
+// counts are invariant to any relabelling (the partial orders pick one
+// representative of every automorphism class whatever the labels); per-view
+// counts are not, so a relabelling must be applied to the whole graph and its
+// .vbmap before views are built.
+void degree_relabel(const Csr& g, bool ascending, int threads, std::vector<uint32_t>* new_of_old, Csr* out);
+
 // Connected random pattern: n uniform in [n_min, n_max], each pair an edge with
 // probability p, rejection-sampled until connected.  Draws come from stream
 // `seed` starting at *counter, which is advanced past the draws used.

@@ -2,11 +2,13 @@
 //
 // Partial matches live in HBM as a "frame": SoA columns of matched data-vertex
 // ids (one u32 column per materialised pattern vertex) plus, per computed but
-// unmaterialised pattern vertex u, a candidate set per path given as
-// (begin u64, length u32) into a u32 pool (the reference keeps an index into a
-// per-parent offsets array instead, src/executor/im_data.h:7-90).  A pool may be
-// the view's own adjacency array: a candidate set that is a contiguous slice of
-// one adjacency list is never copied.
+// unmaterialised pattern vertex u, a sorted candidate set per path given as
+// (address u64, length u32) (the reference keeps an index into a per-parent
+// offsets array instead, src/executor/im_data.h:7-90).  A set may point into the
+// view's adjacency array: a candidate set that is a slice of one adjacency list,
+// or a slice of an earlier set, is never copied; order conditions only narrow
+// the slice, and a set is copied only when a NON_EQUAL value actually occurs in
+// it.
 //
 // All kernels are integer-only.  Intersections are warp-per-path: the warp
 // restricts every backward neighbour's adjacency list to the value window the
@@ -31,10 +33,11 @@ constexpr unsigned kFull = 0xffffffffu;
 struct Frame {
   uint64_t P;                    // number of partial matches
   uint32_t* col[VSGM_MAX_QV];    // materialised columns
-  uint64_t* cbeg[VSGM_MAX_QV];   // candidate-set begin per path
+  uint64_t* cset[VSGM_MAX_QV];   // candidate-set address per path
   uint32_t* clen[VSGM_MAX_QV];   // candidate-set length per path
-  const uint32_t* pool[VSGM_MAX_QV];
 };
+
+__device__ __forceinline__ const uint32_t* set_of(const Frame& f, int u, uint64_t p) { return (const uint32_t*)__ldg(f.cset[u] + p); }
 
 // Everything a kernel needs about one op, small enough to pass by value.
 // Warp kernels load the path's materialised values once (lane i holds the value
@@ -205,28 +208,86 @@ __global__ void k_compute_size(Frame f, OpDesc d, const uint64_t* __restrict__ r
 }
 
 // ---------------------------------------------------------------------------
-// COMPUTE with one backward neighbour and no exclusion: the candidate set is a
-// slice of one adjacency list; record it without copying.
+// narrow: apply d's conditions to one sorted set per path without copying.
+// kFromAdj: the set is the adjacency list of backward neighbour b[0] (COMPUTE
+// with one backward neighbour); otherwise the frame's candidates of d.u
+// (FILTER_COMPUTE, MATERIALIZE with conditions).  Order conditions cut the
+// slice; a NON_EQUAL value found inside it marks the path for copying
+// (copy_ub[p] = slice length, else 0).  *total accumulates the exact survivors.
 // ---------------------------------------------------------------------------
-__global__ void k_compute_slice(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t* __restrict__ beg,
-                                uint32_t* __restrict__ len, unsigned long long* __restrict__ total) {
+template <bool kFromAdj>
+__global__ void k_narrow(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t* __restrict__ out_set,
+                         uint32_t* __restrict__ out_len, uint64_t* __restrict__ copy_ub, unsigned long long* __restrict__ total) {
   const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
   unsigned long long mine = 0;
   for (uint64_t p = tid; p < f.P; p += nthreads) {
     Window w;
     make_window_thread(d, f, p, &w);
-    const uint32_t v = __ldg(f.col[d.b[0]] + p);
-    uint64_t a = __ldg(rp + v), z = __ldg(rp + v + 1);
-    uint64_t s = (w.lo > 0) ? lower_bound(ci, a, z, w.lo) : a;
-    uint64_t e = (w.hi <= 0xffffffffull) ? lower_bound(ci, s, z, w.hi) : z;
+    const uint32_t* base;
+    uint64_t n;
+    if (kFromAdj) {
+      const uint32_t v = __ldg(f.col[d.b[0]] + p);
+      const uint64_t a = __ldg(rp + v);
+      base = ci + a;
+      n = __ldg(rp + v + 1) - a;
+    } else {
+      base = set_of(f, d.u, p);
+      n = __ldg(f.clen[d.u] + p);
+    }
+    uint64_t s = (w.lo > 0) ? lower_bound(base, 0, n, w.lo) : 0;
+    uint64_t e = (w.hi <= 0xffffffffull) ? lower_bound(base, s, n, w.hi) : n;
     if (e < s) e = s;
-    beg[p] = s;
-    len[p] = (uint32_t)(e - s);
-    mine += e - s;
+    uint32_t hits = 0;
+#pragma unroll
+    for (int i = 0; i < VSGM_MAX_QV; i++) {
+      if (w.ne[i] == 0xffffffffu || e == s) continue;
+      uint64_t q = lower_bound(base, s, e, w.ne[i]);
+      hits += (q < e && __ldg(base + q) == w.ne[i]) ? 1u : 0u;
+    }
+    out_set[p] = (uint64_t)(base + s);
+    out_len[p] = (uint32_t)(e - s);
+    copy_ub[p] = hits ? (e - s) : 0;
+    mine += (e - s) - hits;
   }
   for (int o = 16; o > 0; o >>= 1) mine += __shfl_down_sync(kFull, mine, o);
   if (lane_id() == 0 && mine) atomicAdd(total, mine);
+}
+
+// copy the narrowed sets of the marked paths (off[p+1] > off[p]) without the
+// NON_EQUAL values, into pool + off[p]; sets and lengths are updated in place
+__global__ void k_copy_marked(Frame f, OpDesc d, const uint64_t* __restrict__ off, uint32_t* __restrict__ pool, uint64_t* __restrict__ set,
+                              uint32_t* __restrict__ len) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint64_t o = off[p];
+    if (off[p + 1] == o) continue;
+    const uint32_t mine = gather_lane(f, d, p);
+    Window w;
+    make_window(d, mine, &w);
+    const uint32_t* in = (const uint32_t*)set[p];
+    const uint32_t n = len[p];
+    uint32_t* out = pool + o;
+    uint32_t written = 0;
+    for (uint32_t base = 0; base < n; base += kWarp) {
+      const uint32_t k = base + lane;
+      uint32_t c = 0;
+      bool ok = false;
+      if (k < n) {
+        c = __ldg(in + k);
+        ok = ne_ok(w, c);
+      }
+      unsigned mask = __ballot_sync(kFull, ok);
+      if (ok) out[written + __popc(mask & ((1u << lane) - 1))] = c;
+      written += __popc(mask);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      set[p] = (uint64_t)out;
+      len[p] = written;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -234,7 +295,7 @@ __global__ void k_compute_slice(Frame f, OpDesc d, const uint64_t* __restrict__ 
 // ---------------------------------------------------------------------------
 template <int NB>
 __global__ void k_compute_write(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint64_t* __restrict__ off,
-                                uint32_t* __restrict__ pool, uint32_t* __restrict__ len) {
+                                uint32_t* __restrict__ pool, uint64_t* __restrict__ set, uint32_t* __restrict__ len) {
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
   const unsigned lane = lane_id();
   for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
@@ -268,7 +329,10 @@ __global__ void k_compute_write(Frame f, OpDesc d, const uint64_t* __restrict__ 
       if (ok) out[written + __popc(mask & ((1u << lane) - 1))] = c;
       written += __popc(mask);
     }
-    if (lane == 0) len[p] = written;
+    if (lane == 0) {
+      set[p] = (uint64_t)out;
+      len[p] = written;
+    }
   }
 }
 
@@ -306,8 +370,8 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
     const uint32_t* oset = nullptr;
     uint64_t on = 0, ocur = 0;
     if (kOther) {
-      oset = f.pool[d.other] + f.cbeg[d.other][p];
-      on = f.clen[d.other][p];
+      oset = set_of(f, d.other, p);
+      on = __ldg(f.clen[d.other] + p);
     }
     for (uint64_t base = ps; base < pe; base += kWarp) {
       const uint64_t k = base + lane;
@@ -332,38 +396,6 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
   if (lane == 0) {
     if (acc) atomicAdd(total, acc);
     if (kBytes && acc_bytes) atomicAdd(bytes, acc_bytes);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// FILTER: keep the candidates of u that satisfy d's conditions (per path)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool cond_ok(const Window& w, uint32_t c) { return (uint64_t)c >= w.lo && (uint64_t)c < w.hi && ne_ok(w, c); }
-
-__global__ void k_filter(Frame f, OpDesc d, const uint64_t* __restrict__ off, uint32_t* __restrict__ pool, uint32_t* __restrict__ len) {
-  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
-  const unsigned lane = lane_id();
-  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
-    const uint32_t mine = gather_lane(f, d, p);
-    Window w;
-    make_window(d, mine, &w);
-    const uint32_t* in = f.pool[d.u] + f.cbeg[d.u][p];
-    const uint32_t n = f.clen[d.u][p];
-    uint32_t* out = pool + off[p];
-    uint32_t written = 0;
-    for (uint32_t base = 0; base < n; base += kWarp) {
-      const uint32_t k = base + lane;
-      uint32_t c = 0;
-      bool ok = false;
-      if (k < n) {
-        c = __ldg(in + k);
-        ok = cond_ok(w, c);
-      }
-      unsigned mask = __ballot_sync(kFull, ok);
-      if (ok) out[written + __popc(mask & ((1u << lane) - 1))] = c;
-      written += __popc(mask);
-    }
-    if (lane == 0) len[p] = written;
   }
 }
 
@@ -397,11 +429,11 @@ __global__ void k_expand(Frame in, Expand x, const uint64_t* __restrict__ off, u
 #pragma unroll
     for (int i = 0; i < VSGM_MAX_QV; i++)
       if (i < x.nm) out.col[x.m[i]][c] = __ldg(in.col[x.m[i]] + p);
-    out.col[x.u][c] = __ldg(in.pool[x.u] + in.cbeg[x.u][p] + r);
+    out.col[x.u][c] = __ldg(set_of(in, x.u, p) + r);
 #pragma unroll
     for (int i = 0; i < VSGM_MAX_QV; i++)
       if (i < x.ncu) {
-        out.cbeg[x.cu[i]][c] = __ldg(in.cbeg[x.cu[i]] + p);
+        out.cset[x.cu[i]][c] = __ldg(in.cset[x.cu[i]] + p);
         out.clen[x.cu[i]][c] = __ldg(in.clen[x.cu[i]] + p);
       }
   }
@@ -424,8 +456,8 @@ __global__ void k_count_two(Frame f, uint8_t u0, uint8_t u1, uint8_t op, unsigne
   const unsigned lane = lane_id();
   unsigned long long acc = 0;
   for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
-    const uint32_t* a0 = f.pool[u0] + f.cbeg[u0][p];
-    const uint32_t* a1 = f.pool[u1] + f.cbeg[u1][p];
+    const uint32_t* a0 = set_of(f, u0, p);
+    const uint32_t* a1 = set_of(f, u1, p);
     uint64_t n0 = f.clen[u0][p], n1 = f.clen[u1][p];
     const uint32_t *walk = a0, *search = a1;
     uint64_t nw = n0, ns = n1;

@@ -1,0 +1,239 @@
+// pm_pipeline: command-line driver with the reference's flags and output lines
+// (src/app/pattern_matching_pipeline.cu:27-201), over the vsgm C ABI.
+//
+//   pm_pipeline -f <graph.bin> [-m GB] [-p P | -kc k | -km k] [-t threads] [-qs queue]
+//               [-pn producers] [-cn consumers] [-dm 0|1] [-df 0|1] [-dr 0|1] [-ds 0|1] [-dst n]
+//
+// Producers materialise view bins (k-hop halos) on the host into a bounded
+// queue of host buffers; one consumer per GPU uploads each view, matches every
+// plan and accumulates exact counts.  Prints "total count for query i: N" and
+// "finish total time, elapsed_time=Xms" like the reference.
+#include <sys/stat.h>
+#include <sys/time.h>
+
+#include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "vsgm.h"
+
+namespace {
+
+struct Args {
+  std::string file = "./data/com-friendster.ungraph.txt.bin";
+  double mem = 10;
+  int pattern = 1, kc = 0, km = 0, threads = 1, qs = 1, pn = 1, cn = 1, dm = 1, df = 1, dr = 0, ds = 0, dst = 1;
+};
+
+// CommandLine's linear scan (src/common/command_line.h:32-86)
+const char* opt(int argc, char** argv, const char* name) {
+  for (int i = 1; i + 1 < argc; i++)
+    if (std::strcmp(argv[i], name) == 0) return argv[i + 1];
+  return nullptr;
+}
+
+double now_us() {
+  timeval t;
+  gettimeofday(&t, nullptr);
+  return t.tv_sec * 1e6 + t.tv_usec;
+}
+
+struct View {
+  int id = -1;
+  std::vector<uint64_t> row_ptrs;
+  std::vector<uint32_t> cols;
+  std::vector<uint32_t> sources;
+  uint64_t n_cols = 0;
+};
+
+// bounded hand-off between producer and consumer threads
+struct Queue {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<View*> items;
+  size_t cap;
+  bool closed = false;
+  explicit Queue(size_t c) : cap(c) {}
+  void push(View* v) {
+    std::unique_lock<std::mutex> l(mu);
+    cv.wait(l, [&] { return items.size() < cap; });
+    items.push_back(v);
+    cv.notify_all();
+  }
+  View* pop() {
+    std::unique_lock<std::mutex> l(mu);
+    cv.wait(l, [&] { return !items.empty() || closed; });
+    if (items.empty()) return nullptr;
+    View* v = items.front();
+    items.pop_front();
+    cv.notify_all();
+    return v;
+  }
+  void close() {
+    std::lock_guard<std::mutex> l(mu);
+    closed = true;
+    cv.notify_all();
+  }
+};
+
+uint64_t work_of(const std::vector<uint32_t>& src, const uint64_t* rp) {
+  uint64_t s = 0;
+  for (uint32_t v : src) s += rp[v + 1] - rp[v];
+  return s;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  if (argc == 1) return -1;
+  Args a;
+  if (auto v = opt(argc, argv, "-f")) a.file = v;
+  if (auto v = opt(argc, argv, "-m")) a.mem = std::atof(v);
+  if (auto v = opt(argc, argv, "-p")) a.pattern = std::atoi(v);
+  if (auto v = opt(argc, argv, "-kc")) a.kc = std::atoi(v);
+  if (auto v = opt(argc, argv, "-km")) a.km = std::atoi(v);
+  if (auto v = opt(argc, argv, "-t")) a.threads = std::atoi(v);
+  if (auto v = opt(argc, argv, "-qs")) a.qs = std::atoi(v);
+  if (auto v = opt(argc, argv, "-pn")) a.pn = std::atoi(v);
+  if (auto v = opt(argc, argv, "-cn")) a.cn = std::atoi(v);
+  if (auto v = opt(argc, argv, "-dm")) a.dm = std::atoi(v);
+  if (auto v = opt(argc, argv, "-df")) a.df = std::atoi(v);
+  if (auto v = opt(argc, argv, "-dr")) a.dr = std::atoi(v);
+  if (auto v = opt(argc, argv, "-ds")) a.ds = std::atoi(v);
+  if (auto v = opt(argc, argv, "-dst")) a.dst = std::atoi(v);
+  if (a.qs < a.cn || a.pn < 1 || a.cn < 1) {
+    std::fprintf(stderr, "error: need -qs >= -cn >= 1 and -pn >= 1\n");
+    return 1;
+  }
+  std::printf("m: %g t: %d qs: %d pn: %d cn: %d\n", a.mem, a.threads, a.qs, a.pn, a.cn);
+
+  // queries and plans (pattern_matching_pipeline.cu:58-87)
+  std::vector<vsgm_plan> plans;
+  if (a.kc) {
+    plans.resize(1);
+    if (vsgm_plan_clique(a.kc, &plans[0])) return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+  } else if (a.km) {
+    int n = 0;
+    plans.resize(64);
+    if (vsgm_plan_graphlets(a.km, plans.data(), 64, &n)) return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+    plans.resize(n);
+  } else {
+    plans.resize(1);
+    if (vsgm_plan_pattern(a.pattern, &plans[0])) return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+  }
+  int hop = 0;
+  uint64_t root_degree = a.df ? ~0ull : 0;
+  for (auto& p : plans) {
+    hop = std::max(hop, p.hop);
+    if (p.root_degree < root_degree) root_degree = p.root_degree;
+  }
+
+  // graph and view bins (:89-100)
+  uint64_t V = 0, E = 0;
+  uint64_t* rp = nullptr;
+  uint32_t* ci = nullptr;
+  if (vsgm_read_csr_bin(a.file.c_str(), &V, &E, &rp, &ci)) return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+  std::printf("vertex_count=%llu,edge_count=%llu\n", (unsigned long long)V, (unsigned long long)E);
+  std::string vbmap = a.file + "." + std::to_string(hop) + ".hop.vbmap";
+  std::vector<int32_t> bins(V);
+  int32_t n_bins = 0;
+  if (vsgm_read_vbmap(vbmap.c_str(), V, bins.data(), &n_bins)) return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+  std::vector<std::vector<uint32_t>> pool(n_bins);
+  for (uint64_t v = 0; v < V; v++) pool[bins[v]].push_back((uint32_t)v);
+  pool.erase(std::remove_if(pool.begin(), pool.end(), [](const std::vector<uint32_t>& s) { return s.empty(); }), pool.end());
+  if (a.ds) {
+    // ViewBinManager::Split (src/view/view_bin_manager.h:69-134): split the bin
+    // furthest above the mean degree sum into two by alternating sources of
+    // descending degree, until the bin count is a multiple of the consumers
+    int target = ((int)pool.size() / a.cn + a.dst) * a.cn;
+    while ((int)pool.size() < target) {
+      uint64_t sum = 0;
+      for (auto& s : pool) sum += work_of(s, rp);
+      uint64_t avg = sum / pool.size(), best = 0;
+      size_t at = 0;
+      for (size_t i = 0; i < pool.size(); i++) {
+        uint64_t w = work_of(pool[i], rp);
+        if (w >= avg && w - avg > best) best = w - avg, at = i;
+      }
+      std::vector<uint32_t> s = pool[at];
+      std::stable_sort(s.begin(), s.end(), [&](uint32_t x, uint32_t y) { return rp[x + 1] - rp[x] > rp[y + 1] - rp[y]; });
+      std::vector<uint32_t> odd, even;
+      for (size_t i = 0; i < s.size(); i++) (i % 2 ? odd : even).push_back(s[i]);
+      pool.erase(pool.begin() + at);
+      pool.push_back(odd);
+      pool.push_back(even);
+    }
+  }
+  if (a.dr || a.ds)
+    std::stable_sort(pool.begin(), pool.end(), [&](const auto& x, const auto& y) { return work_of(x, rp) > work_of(y, rp); });
+  std::printf("loaded view bin partition file, %zu view bins\n", pool.size());
+
+  const uint64_t cap = std::min<uint64_t>(E, (uint64_t)(a.mem * 1e9 / sizeof(uint32_t)));
+  Queue q(a.qs);
+  std::atomic<size_t> next{0};
+  std::atomic<int> failed{0};
+  std::vector<std::vector<uint64_t>> counts(a.cn, std::vector<uint64_t>(plans.size(), 0));
+
+  double t0 = now_us();
+  std::vector<std::thread> producers, consumers;
+  for (int p = 0; p < a.pn; p++)
+    producers.emplace_back([&] {
+      for (size_t id; (id = next++) < pool.size();) {
+        View* v = new View();
+        v->id = (int)id;
+        v->sources = pool[id];
+        v->row_ptrs.resize(V + 1);
+        v->cols.resize(cap);
+        if (vsgm_view_materialize(V, rp, ci, v->sources.data(), v->sources.size(), hop, root_degree, a.threads, v->row_ptrs.data(), v->cols.data(),
+                                  cap, &v->n_cols)) {
+          std::fprintf(stderr, "error: view %zu: %s\n", id, vsgm_last_error());
+          failed = 1;
+          delete v;
+          continue;
+        }
+        q.push(v);
+      }
+    });
+  for (int c = 0; c < a.cn; c++)
+    consumers.emplace_back([&, c] {
+      vsgm_engine* e = nullptr;
+      if (vsgm_create(c, V, plans.data(), (int)plans.size(), 0, 0, &e)) {
+        std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(nullptr));
+        failed = 1;
+        while (View* v = q.pop()) delete v;  // keep producers moving
+        return;
+      }
+      while (View* v = q.pop()) {
+        int rc = vsgm_transfer_view(e, v->row_ptrs.data(), v->cols.data(), v->n_cols, v->sources.data(), v->sources.size());
+        delete v;  // the host buffers are free once the transfer returns
+        if (!rc && a.dm) rc = vsgm_match(e);
+        if (rc) {
+          std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(e));
+          failed = 1;
+        }
+      }
+      vsgm_get_counts(e, counts[c].data());
+      vsgm_destroy(e);
+    });
+  for (auto& t : producers) t.join();
+  q.close();
+  for (auto& t : consumers) t.join();
+  double t1 = now_us();
+  std::printf("finish total time, elapsed_time=%fms\n", (t1 - t0) / 1000.0);
+  for (size_t i = 0; i < plans.size(); i++) {
+    uint64_t s = 0;
+    for (int c = 0; c < a.cn; c++) s += counts[c][i];
+    std::printf("total count for query %zu: %llu\n", i, (unsigned long long)s);
+  }
+  vsgm_free(rp);
+  vsgm_free(ci);
+  return failed ? 2 : 0;
+}
