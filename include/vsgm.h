@@ -181,6 +181,14 @@ int vsgm_mlp_train_step(vsgm_mlp* m, const float* x, const float* target, const 
 const char* vsgm_mlp_error(vsgm_mlp* m);
 int vsgm_mlp_destroy(vsgm_mlp* m);
 
+/* Engine switches (no reference counterpart):
+ *   "fuse_tail" (default 1): a MATERIALIZE followed by the final COMPUTE_COUNT runs as
+ *   one kernel that stages the parent's shared lists in shared memory instead of
+ *   expanding the children;
+ *   "stage_cap" (default and maximum 1536): largest shared list staged per warp, in
+ *   vertex ids; larger ones take the per-child intersection. */
+int vsgm_set_option(vsgm_engine* e, const char* name, int64_t value);
+
 /* Collect op_ms / op_bytes (adds CUDA events and a small accounting pass). */
 int vsgm_set_profiling(vsgm_engine* e, int on);
 

@@ -160,3 +160,59 @@ def test_batched_run_with_partial_sources(vs, orc, graphs):
     with vs.Engine(g.V, [p]) as e:
         vid = e.add_view(g, src)
         assert e.run_batched([vid]) == [[orc.count(p, g, src)]]
+
+
+@pytest.mark.parametrize("fuse", [0, 1])
+def test_fused_tail_on_and_off(vs, orc, graphs, fuse):
+    """MATERIALIZE + COMPUTE_COUNT fused or expanded: same counts."""
+    g = graphs["chunglu"]
+    plans = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_clique(5), vs.plan_pattern(1), vs.plan_pattern(5),
+             vs.plan_pattern(8), vs.plan_pattern(16), vs.plan_pattern(18)]
+    with vs.Engine(g.V, plans) as e:
+        e.set_option("fuse_tail", fuse)
+        e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+        e.match()
+        assert e.counts() == [orc.count(p, g) for p in plans]
+
+
+def _hub_graph(vs, leaves=2000, chords=3000, seed=4):
+    """One hub joined to every leaf, leaves on a ring plus random chords."""
+    rng = np.random.default_rng(seed)
+    edges = {(0, i) for i in range(1, leaves + 1)}
+    edges |= {(i, i % leaves + 1) for i in range(1, leaves + 1)}
+    for a, b in rng.integers(1, leaves + 1, size=(chords, 2)):
+        if a != b:
+            edges.add((min(a, b), max(a, b)))
+    n = leaves + 1
+    rows = [[] for _ in range(n)]
+    for a, b in edges:
+        rows[a].append(b)
+        rows[b].append(a)
+    rp = np.zeros(n + 1, np.uint64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    return vs.Graph(rp, np.array([x for r in rows for x in sorted(r)], dtype=np.uint32))
+
+
+def test_fused_tail_large_staged_sets(vs, orc, graphs):
+    """Shared lists larger than the stage take the per-child path (natural hub, and forced)."""
+    hub, _ = vs.degree_relabel(_hub_graph(vs))
+    assert hub.degrees().max() > 1536
+    plans = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(8)]
+    for g in (hub, graphs["rmat8"]):
+        want = [orc.count(p, g) for p in plans]
+        for cap in (1536, 16, 0):
+            with vs.Engine(g.V, plans) as e:
+                e.set_option("stage_cap", cap)
+                e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+                e.match()
+                assert e.counts() == want, cap
+
+
+def test_relabelled_graph_same_counts(vs, orc, graphs):
+    g = graphs["rmat8"]
+    plans = [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2)]
+    want = [orc.count(p, g) for p in plans]
+    for asc in (True, False):
+        h, perm = vs.degree_relabel(g, ascending=asc)
+        assert sorted(perm.tolist()) == list(range(g.V))
+        assert vs.count_graph(h, plans) == want

@@ -101,6 +101,8 @@ struct vsgm_engine {
   std::vector<uint64_t> totals;
   std::vector<vsgm_plan_stats> stats;
   bool profiling = false;
+  bool fuse_tail = true;           // fused MATERIALIZE + COMPUTE_COUNT (vsgm_set_option)
+  uint32_t stage_cap = kStageCap;  // shared-memory stage of the fused tail, in u32
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
 
@@ -432,13 +434,105 @@ struct vsgm_engine {
 
   void op_materialize(int i, const Frame& f, int u) {
     const vsgm_plan& p = *plan;
+    const bool fuse = fusable(i, u);
+    auto next = [&](const Frame& g) {
+      if (fuse)
+        fused_count(i, g, u);
+      else
+        materialize_frame(i, g, u);
+    };
     if (p.materialize_cond[u].count > 0) {
       OpDesc d = make_desc(i, p.materialize_cond[u]);
       d.u = (uint8_t)u;
-      narrow_then(i, f, d, false, u, [&](const Frame& g) { materialize_frame(i, g, u); });
+      narrow_then(i, f, d, false, u, next);
     } else {
-      materialize_frame(i, f, u);
+      next(f);
     }
+  }
+
+  // MATERIALIZE(u) directly followed by the final COMPUTE_COUNT(w), u one of w's
+  // backward neighbours: count without expanding the children
+  bool fusable(int i, int u) const {
+    const vsgm_plan& p = *plan;
+    if (!fuse_tail || i + 1 != (int)p.n_ops - 1 || p.op_type[i + 1] != VSGM_COMPUTE_COUNT) return false;
+    const int w = p.op_vertex[i + 1];
+    const vsgm_vgroup& B = p.backward[w];
+    bool has_u = false;
+    for (int k = 0; k < B.count; k++) has_u |= (B.v[k] == u);
+    if (!has_u || B.count < 2 || B.count > 6) return false;
+    if (p.computed_unmat[i + 1].count > 1) return false;
+    int on_u = 0;
+    for (int k = 0; k < p.compute_cond[w].count; k++) on_u += (p.compute_cond[w].v[k] == u);
+    return on_u <= 1;
+  }
+
+  void fused_count(int i, const Frame& f, int u) {
+    const vsgm_plan& p = *plan;
+    const int w = p.op_vertex[i + 1];
+    FusedDesc fd;
+    std::memset(&fd, 0, sizeof(fd));
+    // the known part: materialised[i] columns, B(w) minus u, conditions not on u
+    vsgm_conds known;
+    std::memset(&known, 0, sizeof(known));
+    const vsgm_conds& cc = p.compute_cond[w];
+    for (int k = 0; k < cc.count; k++) {
+      if (cc.v[k] == u) {
+        fd.has_cond_u = 1;
+        fd.cond_u_op = cc.op[k];
+      } else {
+        known.op[known.count] = cc.op[k];
+        known.v[known.count++] = cc.v[k];
+      }
+    }
+    fd.known = make_desc(i, known);
+    fd.known.u = (uint8_t)w;
+    {
+      const vsgm_vgroup& B = p.backward[w];
+      int slot[VSGM_MAX_QV] = {0};
+      for (int k = 0; k < p.materialized[i].count; k++) slot[p.materialized[i].v[k]] = k;
+      fd.known.nb = 0;
+      for (int k = 0; k < B.count; k++)
+        if (B.v[k] != u) {
+          fd.known.b[fd.known.nb] = B.v[k];
+          fd.known.bs[fd.known.nb++] = (uint8_t)slot[B.v[k]];
+        }
+    }
+    fd.u = (uint8_t)u;
+    fd.stage_cap = stage_cap;
+    fd.other = -1;
+    const vsgm_vgroup& cu = p.computed_unmat[i + 1];
+    if (cu.count == 1) {
+      fd.other = (int8_t)cu.v[0];
+      fd.other_op = p.order[w][cu.v[0]];
+    }
+    // children count, for the statistics
+    CK(cudaMemsetAsync(d_bytes + 1, 0, sizeof(unsigned long long), stream));
+    k_count_one<<<grid_threads(f.P), 256, 0, stream>>>(f, (uint8_t)u, d_bytes + 1);
+    CK(cudaGetLastError());
+    const uint64_t children = read_u64((const uint64_t*)(d_bytes + 1));
+    st->op_outputs[i] += children;
+    st->op_paths[i + 1] += children;
+    begin_op();
+    const unsigned g = grid_warps(f.P);
+    const bool other = fd.other >= 0;
+    switch (fd.known.nb) {
+#define VSGM_FUSED(NK)                                                                    \
+  case NK:                                                                                \
+    if (other)                                                                            \
+      k_mat_count<NK, true><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes);  \
+    else                                                                                  \
+      k_mat_count<NK, false><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes); \
+    break;
+      VSGM_FUSED(1)
+      VSGM_FUSED(2)
+      VSGM_FUSED(3)
+      VSGM_FUSED(4)
+      VSGM_FUSED(5)
+#undef VSGM_FUSED
+      default: throw OutOfMemory{"unsupported fused op shape"};
+    }
+    CK(cudaGetLastError());
+    end_op(i + 1, 1);
   }
 
   void materialize_frame(int i, const Frame& f, int u) {
@@ -793,6 +887,21 @@ int vsgm_get_stats(vsgm_engine* e, int plan, vsgm_plan_stats* out) {
   if (!e || !out || plan < 0 || plan >= (int)e->plans.size()) return engine_fail(e, VSGM_EINVAL, "bad stats request");
   *out = e->stats[plan];
   return VSGM_OK;
+}
+
+int vsgm_set_option(vsgm_engine* e, const char* name, int64_t value) {
+  if (!e || !name) return engine_fail(e, VSGM_EINVAL, "null argument");
+  const std::string n(name);
+  if (n == "fuse_tail") {
+    e->fuse_tail = value != 0;
+    return VSGM_OK;
+  }
+  if (n == "stage_cap") {
+    if (value < 0 || value > kStageCap) return engine_fail(e, VSGM_EINVAL, "stage_cap must be 0.." + std::to_string(kStageCap));
+    e->stage_cap = (uint32_t)value;
+    return VSGM_OK;
+  }
+  return engine_fail(e, VSGM_EINVAL, "unknown option " + n);
 }
 
 int vsgm_set_profiling(vsgm_engine* e, int on) {

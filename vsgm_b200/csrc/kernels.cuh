@@ -291,6 +291,87 @@ __global__ void k_copy_marked(Frame f, OpDesc d, const uint64_t* __restrict__ of
 }
 
 // ---------------------------------------------------------------------------
+// Warp intersection of the backward lists of one path.  emit(ok, c) is called by
+// every lane once per step; the lanes with ok hold candidates, in increasing
+// order across lanes and steps.
+//  - merge: when the second-shortest restricted list is at most kMergeRatio
+//    times the shortest, both are streamed 32 at a time (coalesced) and each lane
+//    finds its element of the shortest list in the other's window by a
+//    register binary search over shuffles;
+//  - gallop: otherwise lanes walk the shortest list with stride 32 and gallop
+//    forward in the longer lists.
+// Any remaining lists (three or more backward neighbours) are galloped.
+// ---------------------------------------------------------------------------
+constexpr uint64_t kMergeRatio = 4;
+
+template <int NB, typename Emit>
+__device__ __forceinline__ void intersect_warp(const Window& w, const Lists& L, const uint32_t* __restrict__ ci, Emit&& emit) {
+  const unsigned lane = lane_id();
+  uint64_t pos[NB];
+#pragma unroll
+  for (int j = 0; j < NB; j++) pos[j] = L.s[j];
+  int jb = -1;
+  uint64_t bs = 0, be = 0, blen = ~0ull;
+#pragma unroll
+  for (int j = 0; j < NB; j++)
+    if (j != L.pivot && L.e[j] - L.s[j] < blen) {
+      blen = L.e[j] - L.s[j];
+      bs = L.s[j];
+      be = L.e[j];
+      jb = j;
+    }
+  const uint64_t alen = L.pe - L.ps;
+  if (NB >= 2 && alen >= 64 && blen <= kMergeRatio * alen) {
+    uint64_t ia = L.ps, ib = bs;
+    while (ia < L.pe && ib < be) {
+      const uint32_t nA = (uint32_t)(L.pe - ia < (uint64_t)kWarp ? L.pe - ia : (uint64_t)kWarp);
+      const uint32_t nB = (uint32_t)(be - ib < (uint64_t)kWarp ? be - ib : (uint64_t)kWarp);
+      const uint32_t x = lane < nA ? __ldg(ci + ia + lane) : 0xffffffffu;
+      const uint32_t y = lane < nB ? __ldg(ci + ib + lane) : 0xffffffffu;
+      const uint32_t mA = __shfl_sync(kFull, x, nA - 1), mB = __shfl_sync(kFull, y, nB - 1);
+      const uint32_t m = mA < mB ? mA : mB;
+      int q = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const uint32_t yy = __shfl_sync(kFull, y, q + step - 1);
+        if (yy < x) q += step;
+      }
+      const uint32_t yq = __shfl_sync(kFull, y, q);
+      const bool in_a = lane < nA && x <= m;
+      bool ok = in_a && yq == x && ne_ok(w, x);
+#pragma unroll
+      for (int j = 0; j < NB; j++) {
+        if (j == L.pivot || j == jb || !ok) continue;
+        uint64_t r = gallop(ci, pos[j], L.e[j], x);
+        pos[j] = r;
+        ok = (r < L.e[j]) && (__ldg(ci + r) == x);
+      }
+      emit(ok, x);
+      ia += __popc(__ballot_sync(kFull, in_a));
+      ib += __popc(__ballot_sync(kFull, lane < nB && y <= m));
+    }
+    return;
+  }
+  for (uint64_t base = L.ps; base < L.pe; base += kWarp) {
+    const uint64_t k = base + lane;
+    bool ok = false;
+    uint32_t c = 0xffffffffu;
+    if (k < L.pe) {
+      c = __ldg(ci + k);
+      ok = ne_ok(w, c);
+#pragma unroll
+      for (int j = 0; j < NB; j++) {
+        if (j == L.pivot || !ok) continue;
+        uint64_t r = gallop(ci, pos[j], L.e[j], c);
+        pos[j] = r;
+        ok = (r < L.e[j]) && (__ldg(ci + r) == c);
+      }
+    }
+    emit(ok, c);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // COMPUTE: write the sorted candidate set of every path at pool[off[p]...]
 // ---------------------------------------------------------------------------
 template <int NB>
@@ -304,31 +385,13 @@ __global__ void k_compute_write(Frame f, OpDesc d, const uint64_t* __restrict__ 
     make_window(d, mine, &w);
     Lists L;
     restrict_lists(d, mine, w, rp, ci, &L);
-    const uint64_t ps = L.ps, pe = L.pe;
-    uint64_t pos[NB];
-#pragma unroll
-    for (int j = 0; j < NB; j++) pos[j] = L.s[j];
     uint32_t* out = pool + off[p];
     uint32_t written = 0;
-    for (uint64_t base = ps; base < pe; base += kWarp) {
-      const uint64_t k = base + lane;
-      bool ok = false;
-      uint32_t c = 0;
-      if (k < pe) {
-        c = __ldg(ci + k);
-        ok = ne_ok(w, c);
-#pragma unroll
-        for (int j = 0; j < NB; j++) {
-          if (j == L.pivot || !ok) continue;
-          uint64_t q = gallop(ci, pos[j], L.e[j], c);
-          pos[j] = q;
-          ok = (q < L.e[j]) && (__ldg(ci + q) == c);
-        }
-      }
+    intersect_warp<NB>(w, L, ci, [&](bool ok, uint32_t c) {
       unsigned mask = __ballot_sync(kFull, ok);
       if (ok) out[written + __popc(mask & ((1u << lane) - 1))] = c;
       written += __popc(mask);
-    }
+    });
     if (lane == 0) {
       set[p] = (uint64_t)out;
       len[p] = written;
@@ -362,32 +425,16 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
     make_window(d, mine, &w);
     Lists L;
     restrict_lists(d, mine, w, rp, ci, &L);
-    const uint64_t ps = L.ps, pe = L.pe;
-    if (kBytes && lane == 0) acc_bytes += 4ull * L.full_min + 16ull * NB + 4ull * d.nm;
-    uint64_t pos[NB];
-#pragma unroll
-    for (int j = 0; j < NB; j++) pos[j] = L.s[j];
+    if (kBytes && lane == 0) acc_bytes += 4ull * (L.pe - L.ps) + 16ull * NB + 4ull * d.nm;
     const uint32_t* oset = nullptr;
     uint64_t on = 0, ocur = 0;
     if (kOther) {
       oset = set_of(f, d.other, p);
       on = __ldg(f.clen[d.other] + p);
     }
-    for (uint64_t base = ps; base < pe; base += kWarp) {
-      const uint64_t k = base + lane;
-      if (k < pe) {
-        uint32_t c = __ldg(ci + k);
-        bool ok = ne_ok(w, c);
-#pragma unroll
-        for (int j = 0; j < NB; j++) {
-          if (j == L.pivot || !ok) continue;
-          uint64_t q = gallop(ci, pos[j], L.e[j], c);
-          pos[j] = q;
-          ok = (q < L.e[j]) && (__ldg(ci + q) == c);
-        }
-        if (ok) acc += kOther ? count_vs(oset, on, &ocur, c, d.other_op) : 1ull;
-      }
-    }
+    intersect_warp<NB>(w, L, ci, [&](bool ok, uint32_t c) {
+      if (ok) acc += kOther ? count_vs(oset, on, &ocur, c, d.other_op) : 1ull;
+    });
   }
   for (int o = 16; o > 0; o >>= 1) {
     acc += __shfl_down_sync(kFull, acc, o);
@@ -396,6 +443,242 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
   if (lane == 0) {
     if (acc) atomicAdd(total, acc);
     if (kBytes && acc_bytes) atomicAdd(bytes, acc_bytes);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fused MATERIALIZE(u) + COMPUTE_COUNT(w) over the parent frame.
+//
+// The children of one parent share every backward list of w except N(child), so
+// the warp intersects the parent-known lists once (restricted by the conditions
+// that do not involve u, and by the bound the smallest / largest child puts on
+// w) into shared memory.  Then, one child per lane, every child c in the
+// parent's candidates of u counts |I ∩ N(c)| under its own condition by probing
+// N(c) for the elements of its slice of I; children whose slice is long are
+// redone by the whole warp (walk the shorter side, probe the other).  Parents
+// whose staged set would not fit fall back to a per-child warp intersection.
+// Same result as expanding the children and running COMPUTE_COUNT on them
+// (src/executor/ops/materialize.h, src/executor/ops/compute_count.h).
+// ---------------------------------------------------------------------------
+constexpr int kStageCap = 1536;  // u32 per warp (8 warps: 48 KB of static shared memory per block)
+constexpr uint32_t kLaneSlice = 16;
+
+struct FusedDesc {
+  OpDesc known;        // w's backward lists and conditions that do not involve u (slots into the parent gather)
+  uint8_t u;           // materialised vertex (children)
+  uint8_t has_cond_u;
+  uint8_t cond_u_op;   // condition  candidate(w)  op  c
+  int8_t other;        // computed vertex counted against (-1 none)
+  uint8_t other_op;
+  uint32_t stage_cap;  // <= kStageCap; smaller values force the per-child path
+};
+
+__device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t* a, uint32_t lo, uint32_t hi, uint64_t x) {
+  while (lo < hi) {
+    uint32_t mid = (lo + hi) >> 1;
+    if ((uint64_t)a[mid] < x)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// slice [ia, ib) of the staged set I[0, ni) allowed for child c
+__device__ __forceinline__ void child_slice(const FusedDesc& fd, const Window& w, const uint32_t* I, uint32_t ni, uint32_t c, uint32_t* ia,
+                                            uint32_t* ib) {
+  uint64_t lo = w.lo, hi = w.hi;
+  if (fd.has_cond_u) {
+    if (fd.cond_u_op == VSGM_LARGER_THAN && (uint64_t)c + 1 > lo) lo = (uint64_t)c + 1;
+    if (fd.cond_u_op == VSGM_LESS_THAN && (uint64_t)c < hi) hi = c;
+  }
+  *ia = (lo > 0) ? smem_lower_bound(I, 0, ni, lo) : 0;
+  *ib = (hi <= 0xffffffffull) ? smem_lower_bound(I, *ia, ni, hi) : ni;
+}
+
+template <int NK, bool kOther>
+__global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                                   unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
+  __shared__ uint32_t stage[8][kStageCap];
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  uint32_t* I = stage[threadIdx.x / kWarp];
+  const OpDesc& d = fd.known;
+  const uint32_t excl_child = (fd.has_cond_u && fd.cond_u_op == VSGM_NON_EQUAL) ? 1u : 0u;
+  unsigned long long acc = 0, acc_bytes = 0;
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint32_t* cs = set_of(f, fd.u, p);
+    const uint32_t nc = __ldg(f.clen[fd.u] + p);
+    if (nc == 0) continue;
+    const uint32_t mine = gather_lane(f, d, p);
+    Window w;
+    make_window(d, mine, &w);  // conditions not involving u
+    // the children are sorted: an order condition on u bounds what any child can use
+    Window ws = w;
+    if (fd.has_cond_u && fd.cond_u_op == VSGM_LARGER_THAN) window_add(&ws, VSGM_LARGER_THAN, __ldg(cs), 0);
+    if (fd.has_cond_u && fd.cond_u_op == VSGM_LESS_THAN) window_add(&ws, VSGM_LESS_THAN, __ldg(cs + nc - 1), 0);
+    Lists L;
+    restrict_lists(d, mine, ws, rp, ci, &L);  // the NK parent-known lists
+    const uint32_t* oset = nullptr;
+    uint32_t on = 0;
+    if (kOther) {
+      oset = set_of(f, fd.other, p);
+      on = __ldg(f.clen[fd.other] + p);
+    }
+    if ((L.pe - L.ps) <= (uint64_t)fd.stage_cap) {
+      // stage I = intersection of the known lists (NON_EQUAL vs parent values applied)
+      uint32_t ni = 0;
+      if (NK == 1) {
+        for (uint64_t base = L.ps; base < L.pe; base += kWarp) {
+          const uint64_t k = base + lane;
+          uint32_t c = 0;
+          bool ok = false;
+          if (k < L.pe) {
+            c = __ldg(ci + k);
+            ok = ne_ok(w, c);
+          }
+          unsigned mask = __ballot_sync(kFull, ok);
+          if (ok) I[ni + __popc(mask & ((1u << lane) - 1))] = c;
+          ni += __popc(mask);
+        }
+      } else {
+        intersect_warp<NK>(w, L, ci, [&](bool ok, uint32_t c) {
+          unsigned mask = __ballot_sync(kFull, ok);
+          if (ok) I[ni + __popc(mask & ((1u << lane) - 1))] = c;
+          ni += __popc(mask);
+        });
+      }
+      __syncwarp();
+      if (lane == 0) acc_bytes += 4ull * (L.pe - L.ps) + 16ull * NK + 4ull * d.nm;
+      if (ni == 0) continue;
+      for (uint32_t k0 = 0; k0 < nc; k0 += kWarp) {
+        // pass 1, one child per lane; long slices are left for pass 2
+        const uint32_t k = k0 + lane;
+        bool heavy = false;
+        if (k < nc) {
+          const uint32_t c = __ldg(cs + k);
+          uint32_t ia, ib;
+          child_slice(fd, w, I, ni, c, &ia, &ib);
+          if (ib - ia > kLaneSlice) {
+            heavy = true;
+          } else if (ia < ib) {
+            const uint64_t a0 = __ldg(rp + c), z0 = __ldg(rp + c + 1);
+            const uint32_t excl = excl_child ? c : 0xffffffffu;
+            uint64_t cur = a0, ocur = 0;
+            acc_bytes += 4ull * (ib - ia) + 16ull;
+            for (uint32_t j = ia; j < ib; j++) {
+              const uint32_t x = I[j];
+              const uint64_t r = gallop(ci, cur, z0, x);
+              cur = r;
+              if (r < z0 && __ldg(ci + r) == x && x != excl) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
+            }
+          }
+        }
+        // pass 2: the long slices of this group, one child at a time, by the whole warp
+        unsigned todo = __ballot_sync(kFull, heavy);
+        while (todo) {
+          const int src = __ffs(todo) - 1;
+          todo &= todo - 1;
+          const uint32_t c = __ldg(cs + k0 + src);
+          uint32_t ia, ib;
+          child_slice(fd, w, I, ni, c, &ia, &ib);
+          const uint64_t a0 = __ldg(rp + c), z0 = __ldg(rp + c + 1);
+          const uint64_t s2 = lower_bound(ci, a0, z0, I[ia]);
+          const uint64_t e2 = lower_bound(ci, s2, z0, (uint64_t)I[ib - 1] + 1);
+          if (lane == 0) acc_bytes += 4ull * ((uint64_t)(ib - ia) < e2 - s2 ? (uint64_t)(ib - ia) : e2 - s2) + 16ull;
+          if (s2 >= e2) continue;
+          const uint32_t excl = excl_child ? c : 0xffffffffu;
+          uint64_t ocur = 0;
+          if ((uint64_t)(ib - ia) <= (e2 - s2)) {
+            uint64_t cur = s2;
+            for (uint32_t j = ia + lane; j < ib; j += kWarp) {
+              const uint32_t x = I[j];
+              const uint64_t r = gallop(ci, cur, e2, x);
+              cur = r;
+              if (r < e2 && __ldg(ci + r) == x && x != excl) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
+            }
+          } else {
+            uint32_t cur = ia;
+            for (uint64_t j = s2 + lane; j < e2; j += kWarp) {
+              const uint32_t x = __ldg(ci + j);
+              const uint32_t r = smem_lower_bound(I, cur, ib, x);
+              cur = r;
+              if (r < ib && I[r] == x && x != excl) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
+            }
+          }
+        }
+      }
+    } else {
+      // too large to stage: per child, intersect the known lists with N(c)
+      for (uint32_t k = 0; k < nc; k++) {
+        const uint32_t c = __ldg(cs + k);
+        Window wc = w;
+        if (fd.has_cond_u && fd.cond_u_op == VSGM_NON_EQUAL) {
+          // the known conditions leave at least one NON_EQUAL slot free
+          bool placed = false;
+#pragma unroll
+          for (int q = VSGM_MAX_QV - 1; q >= 0; q--)
+            if (!placed && wc.ne[q] == 0xffffffffu) {
+              wc.ne[q] = c;
+              placed = true;
+            }
+        } else if (fd.has_cond_u) {
+          window_add(&wc, fd.cond_u_op, c, 0);
+        }
+        // lanes < NK: the known lists; lane NK: N(c)
+        uint64_t ls = 0, le = 0;
+#pragma unroll
+        for (int q = 0; q < VSGM_MAX_QV; q++)
+          if (q < NK && q == (int)lane) {
+            ls = L.s[q];
+            le = L.e[q];
+          }
+        if (lane == NK) {
+          ls = __ldg(rp + c);
+          le = __ldg(rp + c + 1);
+        }
+        if (lane <= NK) {
+          const uint64_t z = le;
+          ls = (wc.lo > 0) ? lower_bound(ci, ls, z, wc.lo) : ls;
+          le = (wc.hi <= 0xffffffffull) ? lower_bound(ci, ls, z, wc.hi) : z;
+          if (le < ls) le = ls;
+        }
+        Lists Lc;
+        uint64_t best = ~0ull;
+        int piv = 0;
+#pragma unroll
+        for (int q = 0; q < VSGM_MAX_QV; q++) {
+          const uint64_t sq = __shfl_sync(kFull, ls, q), eq = __shfl_sync(kFull, le, q);
+          Lc.s[q] = sq;
+          Lc.e[q] = eq;
+          if (q <= NK && eq - sq < best) {
+            best = eq - sq;
+            piv = q;
+          }
+        }
+        Lc.pivot = piv;
+        Lc.ps = Lc.pe = 0;
+#pragma unroll
+        for (int q = 0; q < VSGM_MAX_QV; q++)
+          if (q == piv) {
+            Lc.ps = Lc.s[q];
+            Lc.pe = Lc.e[q];
+          }
+        if (lane == 0) acc_bytes += 4ull * (Lc.pe - Lc.ps) + 16ull * (NK + 1);
+        uint64_t ocur = 0;
+        intersect_warp<NK + 1>(wc, Lc, ci, [&](bool ok, uint32_t x) {
+          if (ok) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
+        });
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    acc += __shfl_down_sync(kFull, acc, o);
+    acc_bytes += __shfl_down_sync(kFull, acc_bytes, o);
+  }
+  if (lane == 0) {
+    if (acc) atomicAdd(total, acc);
+    if (bytes && acc_bytes) atomicAdd(bytes, acc_bytes);
   }
 }
 
