@@ -154,6 +154,13 @@ int vsgm_add_view(vsgm_engine* e, uint64_t V, const uint64_t* row_ptrs, const ui
                   uint64_t n_sources, int* view_id);
 int vsgm_run_batched(vsgm_engine* e, const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* counts);
 
+/* vsgm_run_batched plus, per (plan, view) pair: level_paths[pair * VSGM_MAX_OPS + i]
+ * = partial matches entering op i (the intermediate sizes the learned planner is
+ * trained on), and with step_budget > 0 every task stops after that many steps and
+ * sets overflow[pair] (its counts are then partial).  Either output may be NULL. */
+int vsgm_run_batched_ex(vsgm_engine* e, const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t step_budget, uint64_t* counts,
+                        uint64_t* level_paths, uint32_t* overflow);
+
 typedef struct vsgm_batch_stats {
   uint64_t tasks;         /* root-range tasks in the last batched run */
   uint64_t launches;      /* kernels launched by it */

@@ -216,3 +216,20 @@ def test_relabelled_graph_same_counts(vs, orc, graphs):
         h, perm = vs.degree_relabel(g, ascending=asc)
         assert sorted(perm.tolist()) == list(range(g.V))
         assert vs.count_graph(h, plans) == want
+
+
+def test_batched_level_paths_and_step_budget(vs, orc, graphs):
+    """Per-op partial-match counts of the persistent run equal the oracle's; a step budget stops tasks."""
+    g = graphs["rmat7"]
+    plans = [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(3), vs.plan_pattern(13)]
+    with vs.Engine(g.V, plans) as e:
+        vid = e.add_view(g)
+        cnt, lvl, ovf = e.run_batched_ex([vid])
+        for i, p in enumerate(plans):
+            total, paths = orc.op_paths(p, g)
+            assert int(cnt[i][0]) == total
+            assert [int(x) for x in lvl[i][0][:p.n_ops]] == paths
+        assert not ovf.any()
+        cnt2, _, ovf2 = e.run_batched_ex([vid], step_budget=5)
+        assert ovf2.all()
+        assert all(int(cnt2[i][0]) <= int(cnt[i][0]) for i in range(len(plans)))

@@ -244,6 +244,19 @@ class Engine:
         capi.check(_L().vsgm_run_batched(self.h, v, len(view_ids), p, len(plan_ids), capi.ptr(out, C.c_uint64)), self.h)
         return [[int(x) for x in out[i * len(view_ids):(i + 1) * len(view_ids)]] for i in range(len(plan_ids))]
 
+    def run_batched_ex(self, view_ids, plan_ids=None, step_budget=0):
+        """Counts [plan][view], level paths [plan][view][op] and overflow flags [plan][view]."""
+        plan_ids = list(range(len(self.plans))) if plan_ids is None else list(plan_ids)
+        nv, npl = len(view_ids), len(plan_ids)
+        v = (C.c_int * nv)(*view_ids)
+        p = (C.c_int * npl)(*plan_ids)
+        cnt = np.zeros(npl * nv, np.uint64)
+        lvl = np.zeros(npl * nv * capi.MAX_OPS, np.uint64)
+        ovf = np.zeros(npl * nv, np.uint32)
+        capi.check(_L().vsgm_run_batched_ex(self.h, v, nv, p, npl, step_budget, capi.ptr(cnt, C.c_uint64), capi.ptr(lvl, C.c_uint64),
+                                            capi.ptr(ovf, C.c_uint32)), self.h)
+        return cnt.reshape(npl, nv), lvl.reshape(npl, nv, capi.MAX_OPS), ovf.reshape(npl, nv)
+
     def batch_stats(self):
         s = capi.BatchStats()
         capi.check(_L().vsgm_get_batch_stats(self.h, C.byref(s)), self.h)

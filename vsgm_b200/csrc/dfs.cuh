@@ -187,12 +187,19 @@ __device__ __forceinline__ bool dfs_has_ne(const uint32_t* a, uint32_t n, const 
 // means a candidate set did not fit in cap (the host reports an error; cap is
 // the largest degree, which bounds every candidate set, so it does not happen).
 // Nothing in the kernel waits on another warp.
+// Optional outputs: level_paths[pair * VSGM_MAX_OPS + i] += partial matches
+// entering op i (pair = plan * n_views + view); with step_budget > 0 a task stops
+// after that many forward steps and sets overflow[pair] (its counts are then
+// partial) - a bound on the work of one launch, not a wait.
 __global__ void __launch_bounds__(kDfsWarps * kWarp) k_dfs(const DfsPlan* __restrict__ plans, const DfsView* __restrict__ views,
                                                            const DfsTask* __restrict__ tasks, uint64_t n_tasks, unsigned long long* __restrict__ head,
                                                            uint32_t* __restrict__ scratch, uint64_t cap, uint32_t levels, uint32_t n_views,
-                                                           unsigned long long* __restrict__ counts, unsigned int* __restrict__ status) {
+                                                           unsigned long long* __restrict__ counts, unsigned int* __restrict__ status,
+                                                           unsigned long long* __restrict__ level_paths, uint64_t step_budget,
+                                                           unsigned int* __restrict__ overflow) {
   __shared__ DfsState sst[kDfsWarps];
   __shared__ DfsOp sop[kDfsWarps][VSGM_MAX_OPS];
+  __shared__ unsigned long long svisit[kDfsWarps][VSGM_MAX_OPS];
   const unsigned lane = lane_id(), wib = threadIdx.x / kWarp;
   DfsState& S = sst[wib];
   DfsOp* O = sop[wib];
@@ -210,15 +217,28 @@ __global__ void __launch_bounds__(kDfsWarps * kWarp) k_dfs(const DfsPlan* __rest
     const uint32_t n_ops = P.n_ops;
     // stage the plan's ops in shared memory
     for (uint32_t i = lane; i < n_ops * (uint32_t)sizeof(DfsOp); i += kWarp) ((uint8_t*)O)[i] = ((const uint8_t*)P.op)[i];
+    if (lane < VSGM_MAX_OPS) svisit[wib][lane] = 0;
     __syncwarp();
     unsigned long long acc = 0;
+    uint64_t steps = 0;
+    bool stopped = false;
 
-    for (uint64_t r = task.r0; r < task.r1; r++) {
-      if (lane == 0) S.M[P.root] = __ldg(V.sources + r);
+    for (uint64_t r = task.r0; r < task.r1 && !stopped; r++) {
+      if (lane == 0) {
+        S.M[P.root] = __ldg(V.sources + r);
+        svisit[wib][0]++;
+      }
       __syncwarp();
       int lvl = 1;
       bool forward = true;
       while (lvl >= 1) {
+        if (forward) {
+          if (lane == 0) svisit[wib][lvl]++;
+          if (step_budget && ++steps > step_budget) {
+            stopped = true;
+            break;
+          }
+        }
         if (!forward) {
           // backtrack: undo FILTER levels, resume the nearest MATERIALIZE
           const DfsOp& o = O[lvl];
@@ -380,7 +400,11 @@ __global__ void __launch_bounds__(kDfsWarps * kWarp) k_dfs(const DfsPlan* __rest
       }
     }
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(kFull, acc, off);
-    if (lane == 0 && acc) atomicAdd(counts + (uint64_t)task.plan * n_views + task.view, acc);
+    const uint64_t pair = (uint64_t)task.plan * n_views + task.view;
+    if (lane == 0 && acc) atomicAdd(counts + pair, acc);
+    if (lane == 0 && stopped && overflow) atomicOr(overflow + pair, 1u);
+    __syncwarp();
+    if (level_paths && lane < n_ops && svisit[wib][lane]) atomicAdd(level_paths + pair * VSGM_MAX_OPS + lane, svisit[wib][lane]);
     __syncwarp();
   }
 }

@@ -631,7 +631,8 @@ struct vsgm_engine {
 
   // One persistent launch over every (plan, view) pair: tasks are root ranges of
   // balanced estimated cost, longest first, popped by warps from a device queue.
-  void run_batched(const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* out) {
+  void run_batched(const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* out, uint64_t* level_out = nullptr,
+                   uint64_t step_budget = 0, uint32_t* overflow_out = nullptr) {
     std::vector<DfsPlan> hp(n_plans);
     uint32_t levels = 1;
     for (int k = 0; k < n_plans; k++) {
@@ -677,7 +678,12 @@ struct vsgm_engine {
     DfsPlan* d_plans = arena.take_n<DfsPlan>(n_plans, "batched plans");
     DfsView* d_views = arena.take_n<DfsView>(n_views, "batched views");
     DfsTask* d_tasks = arena.take_n<DfsTask>(std::max<size_t>(1, ht.size()), "batched tasks");
-    unsigned long long* d_cnt = arena.take_n<unsigned long long>((uint64_t)n_plans * n_views + 2, "batched counts");
+    const uint64_t pairs = (uint64_t)n_plans * n_views;
+    unsigned long long* d_cnt = arena.take_n<unsigned long long>(pairs + 2, "batched counts");
+    unsigned long long* d_lvl = level_out ? arena.take_n<unsigned long long>(pairs * VSGM_MAX_OPS, "level paths") : nullptr;
+    unsigned int* d_ovf = overflow_out ? arena.take_n<unsigned int>(pairs, "overflow flags") : nullptr;
+    if (d_lvl) CK(cudaMemsetAsync(d_lvl, 0, sizeof(unsigned long long) * pairs * VSGM_MAX_OPS, stream));
+    if (d_ovf) CK(cudaMemsetAsync(d_ovf, 0, sizeof(unsigned int) * pairs, stream));
     const uint64_t grid = (uint64_t)sms * 2;
     uint32_t* scratch = arena.take_n<uint32_t>(grid * kDfsWarps * levels * cap, "per-warp scratch");
     CK(cudaMemcpyAsync(d_plans, hp.data(), sizeof(DfsPlan) * n_plans, cudaMemcpyHostToDevice, stream));
@@ -688,7 +694,7 @@ struct vsgm_engine {
     unsigned int* d_status = (unsigned int*)(d_head + 1);
     if (profiling) CK(cudaEventRecord(ev0, stream));
     k_dfs<<<(unsigned)grid, kDfsWarps * kWarp, 0, stream>>>(d_plans, d_views, d_tasks, ht.size(), d_head, scratch, cap, levels, (uint32_t)n_views, d_cnt,
-                                                             d_status);
+                                                             d_status, d_lvl, step_budget, d_ovf);
     CK(cudaGetLastError());
     if (profiling) CK(cudaEventRecord(ev1, stream));
     std::vector<uint64_t> hc((uint64_t)n_plans * n_views + 2);
@@ -705,6 +711,8 @@ struct vsgm_engine {
       bstats.ms = ms;
     }
     for (uint64_t k = 0; k < (uint64_t)n_plans * n_views; k++) out[k] = hc[k];
+    if (level_out) CK(cudaMemcpy(level_out, d_lvl, sizeof(uint64_t) * pairs * VSGM_MAX_OPS, cudaMemcpyDeviceToHost));
+    if (overflow_out) CK(cudaMemcpy(overflow_out, d_ovf, sizeof(uint32_t) * pairs, cudaMemcpyDeviceToHost));
   }
 
   void run_plan(int pi) {
@@ -951,6 +959,20 @@ int vsgm_run_batched(vsgm_engine* e, const int* view_ids, int n_views, const int
     CK(cudaSetDevice(e->device));
     e->arena.top = 0;
     e->run_batched(view_ids, n_views, plan_ids, n_plans, counts);
+  });
+}
+
+int vsgm_run_batched_ex(vsgm_engine* e, const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t step_budget, uint64_t* counts,
+                        uint64_t* level_paths, uint32_t* overflow) {
+  if (!e || !view_ids || !plan_ids || !counts || n_views < 1 || n_plans < 1) return engine_fail(e, VSGM_EINVAL, "bad batched request");
+  for (int k = 0; k < n_views; k++)
+    if (view_ids[k] < 0 || view_ids[k] >= (int)e->rviews.size()) return engine_fail(e, VSGM_EINVAL, "unknown view id");
+  for (int k = 0; k < n_plans; k++)
+    if (plan_ids[k] < 0 || plan_ids[k] >= (int)e->plans.size()) return engine_fail(e, VSGM_EINVAL, "unknown plan id");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    e->arena.top = 0;
+    e->run_batched(view_ids, n_views, plan_ids, n_plans, counts, level_paths, step_budget, overflow);
   });
 }
 
