@@ -178,7 +178,8 @@ def main():
 
     g, plans = make_workload(vs, scale=args.scale, relabel=args.relabel)
     # roots of this rank: a strided share of the vertices (one view per rank)
-    roots = np.arange(rank, g.V, world, dtype=np.uint32)
+    from vsgm_b200.shard import allreduce_counts, roots_of_rank
+    roots = roots_of_rank(g.V, rank, world)
     eng = vs.Engine(g.V, plans, device=local)
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
 
@@ -216,9 +217,7 @@ def main():
         t = torch.tensor([step_ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         step_ms = float(t.item())
-        ct = torch.tensor(counts, dtype=torch.int64, device="cuda")
-        torch.distributed.all_reduce(ct)
-        counts = [int(x) for x in ct.tolist()]
+        counts = allreduce_counts(counts, device="cuda")
     matches = sum(counts)
     value = matches / (step_ms / 1e3)
 

@@ -188,12 +188,20 @@ int vsgm_mlp_train_step(vsgm_mlp* m, const float* x, const float* target, const 
 const char* vsgm_mlp_error(vsgm_mlp* m);
 int vsgm_mlp_destroy(vsgm_mlp* m);
 
-/* Engine switches (no reference counterpart):
+/* Tuning knobs (no reference counterpart), for every plan or for one plan:
  *   "fuse_tail" (default 1): a MATERIALIZE followed by the final COMPUTE_COUNT runs as
  *   one kernel that stages the parent's shared lists in shared memory instead of
  *   expanding the children;
  *   "stage_cap" (default and maximum 1536): largest shared list staged per warp, in
- *   vertex ids; larger ones take the per-child intersection. */
+ *   vertex ids; larger ones take the per-child intersection;
+ *   "merge_ratio" (default 4): two lists whose restricted lengths are within this
+ *   ratio are intersected by a coalesced merge, otherwise by galloping (0: always
+ *   gallop);
+ *   "root_stride" (engine-wide, default 1): match only every k-th source of the view
+ *   (the autotuner's samples; counts are then those of the sample);
+ *   "only_plan" (engine-wide, default -1): vsgm_match runs only this plan.
+ * fuse_tail, stage_cap and merge_ratio never change a count. */
+int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t value);
 int vsgm_set_option(vsgm_engine* e, const char* name, int64_t value);
 
 /* Collect op_ms / op_bytes (adds CUDA events and a small accounting pass). */

@@ -233,3 +233,27 @@ def test_batched_level_paths_and_step_budget(vs, orc, graphs):
         cnt2, _, ovf2 = e.run_batched_ex([vid], step_budget=5)
         assert ovf2.all()
         assert all(int(cnt2[i][0]) <= int(cnt[i][0]) for i in range(len(plans)))
+
+
+def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
+    """Every intersection variant / fusion setting gives the same counts; the autotuner picks one."""
+    from vsgm_b200.autotune import autotune
+    g = graphs["rmat8"]
+    plans = [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2), vs.plan_pattern(4)]
+    want = [orc.count(p, g) for p in plans]
+    with vs.Engine(g.V, plans) as e:
+        e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+        for ratio in (0, 1, 2, 64):
+            e.set_option("merge_ratio", ratio)
+            e.reset_counts()
+            e.match()
+            assert e.counts() == want, ratio
+        report = autotune(e, len(plans), stride=4)
+        assert [r["plan"] for r in report] == list(range(len(plans)))
+        e.match()
+        assert e.counts() == want
+        e.set_option("root_stride", 3)
+        e.set_option("only_plan", 1)
+        e.reset_counts()
+        e.match()
+        assert e.counts()[1] == orc.count(plans[1], g, np.arange(0, g.V, 3, dtype=np.uint32))

@@ -262,8 +262,11 @@ class Engine:
         capi.check(_L().vsgm_get_batch_stats(self.h, C.byref(s)), self.h)
         return s
 
-    def set_option(self, name, value):
-        capi.check(_L().vsgm_set_option(self.h, name.encode(), int(value)), self.h)
+    def set_option(self, name, value, plan=None):
+        if plan is None:
+            capi.check(_L().vsgm_set_option(self.h, name.encode(), int(value)), self.h)
+        else:
+            capi.check(_L().vsgm_set_plan_option(self.h, int(plan), name.encode(), int(value)), self.h)
 
     def set_profiling(self, on=True):
         capi.check(_L().vsgm_set_profiling(self.h, 1 if on else 0), self.h)

@@ -1,0 +1,59 @@
+"""Autotuner for the engine's per-plan knobs (intersection variant and tail fusion).
+
+For every plan it times each candidate setting of (fuse_tail, merge_ratio,
+stage_cap) on a strided sample of the view's roots (engine option root_stride)
+and keeps the fastest; the choice is written back as per-plan options.  Counts
+never depend on these knobs, so tuning on a sample is safe; the sample only has
+to rank the settings.
+"""
+import itertools
+import time
+
+CANDIDATES = {
+    "fuse_tail": (1, 0),
+    "merge_ratio": (0, 2, 4, 16),
+    "stage_cap": (1536, 384),
+}
+
+
+def _settings(space):
+    keys = list(space)
+    for vals in itertools.product(*(space[k] for k in keys)):
+        cfg = dict(zip(keys, vals))
+        if not cfg["fuse_tail"] and cfg["stage_cap"] != space["stage_cap"][0]:
+            continue  # the stage only matters for the fused tail
+        yield cfg
+
+
+def autotune(engine, n_plans, stride=64, space=None):
+    """Tune every plan of an engine whose view is already transferred; returns
+    [{"plan": i, "best": cfg, "ms": {cfg-key: ms}}] and applies the best settings."""
+    space = space or CANDIDATES
+    report = []
+    engine.set_profiling(True)
+    engine.set_option("root_stride", stride)
+    try:
+        for i in range(n_plans):
+            engine.set_option("only_plan", i)
+            timings = {}
+            best, best_ms = None, float("inf")
+            for cfg in _settings(space):
+                for k, v in cfg.items():
+                    engine.set_option(k, v, plan=i)
+                t = time.perf_counter()
+                engine.match()
+                wall = (time.perf_counter() - t) * 1e3
+                s = engine.stats(i)
+                ms = sum(s.op_ms[j] for j in range(len(s.op_ms))) or wall
+                key = ",".join(f"{k}={v}" for k, v in cfg.items())
+                timings[key] = ms
+                if ms < best_ms:
+                    best, best_ms = cfg, ms
+            for k, v in best.items():
+                engine.set_option(k, v, plan=i)
+            report.append({"plan": i, "best": best, "ms": timings})
+    finally:
+        engine.set_option("only_plan", -1)
+        engine.set_option("root_stride", 1)
+        engine.reset_counts()
+    return report

@@ -101,8 +101,16 @@ struct vsgm_engine {
   std::vector<uint64_t> totals;
   std::vector<vsgm_plan_stats> stats;
   bool profiling = false;
-  bool fuse_tail = true;           // fused MATERIALIZE + COMPUTE_COUNT (vsgm_set_option)
-  uint32_t stage_cap = kStageCap;  // shared-memory stage of the fused tail, in u32
+  // per-plan tuning knobs (vsgm_set_option / vsgm_set_plan_option)
+  struct Knobs {
+    bool fuse_tail = true;           // fused MATERIALIZE + COMPUTE_COUNT
+    uint32_t stage_cap = kStageCap;  // shared-memory stage of the fused tail, in u32
+    uint32_t merge_ratio = 4;        // merge vs gallop threshold of the warp intersection
+  };
+  std::vector<Knobs> knobs;
+  Knobs cur;
+  uint64_t root_stride = 1;  // >1: match only every root_stride-th source (autotuning samples)
+  int only_plan = -1;        // >=0: vsgm_match runs this plan only
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
 
@@ -217,6 +225,7 @@ struct vsgm_engine {
     std::memset(&d, 0, sizeof(d));
     d.u = p.op_vertex[i];
     d.other = -1;
+    d.merge_ratio = (uint16_t)cur.merge_ratio;
     const vsgm_vgroup& mg = p.materialized[i];
     d.nm = mg.count;
     int slot[VSGM_MAX_QV];
@@ -454,7 +463,7 @@ struct vsgm_engine {
   // backward neighbours: count without expanding the children
   bool fusable(int i, int u) const {
     const vsgm_plan& p = *plan;
-    if (!fuse_tail || i + 1 != (int)p.n_ops - 1 || p.op_type[i + 1] != VSGM_COMPUTE_COUNT) return false;
+    if (!cur.fuse_tail || i + 1 != (int)p.n_ops - 1 || p.op_type[i + 1] != VSGM_COMPUTE_COUNT) return false;
     const int w = p.op_vertex[i + 1];
     const vsgm_vgroup& B = p.backward[w];
     bool has_u = false;
@@ -498,7 +507,7 @@ struct vsgm_engine {
         }
     }
     fd.u = (uint8_t)u;
-    fd.stage_cap = stage_cap;
+    fd.stage_cap = cur.stage_cap;
     fd.other = -1;
     const vsgm_vgroup& cu = p.computed_unmat[i + 1];
     if (cu.count == 1) {
@@ -718,14 +727,24 @@ struct vsgm_engine {
   void run_plan(int pi) {
     plan = &plans[pi];
     st = &stats[pi];
+    cur = knobs[pi];
     d_total = d_counts + pi;
     if (n_src == 0) return;
     Frame f;
     std::memset(&f, 0, sizeof(f));
     f.P = n_src;
     f.col[plan->op_vertex[0]] = d_src;
-    st->op_paths[0] += n_src;
-    st->op_outputs[0] += n_src;
+    Mark m(arena);
+    if (root_stride > 1) {
+      // sampled run: every root_stride-th source only
+      f.P = (n_src + root_stride - 1) / root_stride;
+      uint32_t* sampled = arena.take_n<uint32_t>(f.P, "sampled roots");
+      k_stride_copy<<<grid_threads(f.P), 256, 0, stream>>>(d_src, f.P, root_stride, sampled);
+      CK(cudaGetLastError());
+      f.col[plan->op_vertex[0]] = sampled;
+    }
+    st->op_paths[0] += f.P;
+    st->op_outputs[0] += f.P;
     process(1, f);
     if (profiling) {
       // the CC kernel accumulated algorithmic bytes
@@ -780,6 +799,7 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
   e->max_sources = max_sources;
   e->totals.assign(n_plans, 0);
   e->stats.assign(n_plans, vsgm_plan_stats{});
+  e->knobs.assign(n_plans, vsgm_engine::Knobs{});
   int rc = guarded(e, [&] {
     CK(cudaSetDevice(device));
     CK(cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, device));
@@ -861,6 +881,7 @@ int vsgm_match(vsgm_engine* e) {
     const int n = (int)e->plans.size();
     CK(cudaMemsetAsync(e->d_counts, 0, sizeof(unsigned long long) * (n + 2), e->stream));
     for (int k = 0; k < n; k++) {
+      if (e->only_plan >= 0 && k != e->only_plan) continue;
       e->stats[k] = vsgm_plan_stats{};
       e->arena.top = 0;
       e->arena.peak = 0;
@@ -897,20 +918,39 @@ int vsgm_get_stats(vsgm_engine* e, int plan, vsgm_plan_stats* out) {
   return VSGM_OK;
 }
 
-int vsgm_set_option(vsgm_engine* e, const char* name, int64_t value) {
+int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t value) {
   if (!e || !name) return engine_fail(e, VSGM_EINVAL, "null argument");
+  if (plan < -1 || plan >= (int)e->plans.size()) return engine_fail(e, VSGM_EINVAL, "bad plan index");
   const std::string n(name);
+  const int lo = plan < 0 ? 0 : plan, hi = plan < 0 ? (int)e->plans.size() : plan + 1;
   if (n == "fuse_tail") {
-    e->fuse_tail = value != 0;
+    for (int k = lo; k < hi; k++) e->knobs[k].fuse_tail = value != 0;
     return VSGM_OK;
   }
   if (n == "stage_cap") {
     if (value < 0 || value > kStageCap) return engine_fail(e, VSGM_EINVAL, "stage_cap must be 0.." + std::to_string(kStageCap));
-    e->stage_cap = (uint32_t)value;
+    for (int k = lo; k < hi; k++) e->knobs[k].stage_cap = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "merge_ratio") {
+    if (value < 0 || value > 65535) return engine_fail(e, VSGM_EINVAL, "merge_ratio must be 0..65535");
+    for (int k = lo; k < hi; k++) e->knobs[k].merge_ratio = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "only_plan") {
+    if (value < -1 || value >= (int64_t)e->plans.size()) return engine_fail(e, VSGM_EINVAL, "only_plan must be -1 or a plan index");
+    e->only_plan = (int)value;
+    return VSGM_OK;
+  }
+  if (n == "root_stride") {
+    if (value < 1) return engine_fail(e, VSGM_EINVAL, "root_stride must be >= 1");
+    e->root_stride = (uint64_t)value;
     return VSGM_OK;
   }
   return engine_fail(e, VSGM_EINVAL, "unknown option " + n);
 }
+
+int vsgm_set_option(vsgm_engine* e, const char* name, int64_t value) { return vsgm_set_plan_option(e, -1, name, value); }
 
 int vsgm_set_profiling(vsgm_engine* e, int on) {
   if (!e) return engine_fail(nullptr, VSGM_EINVAL, "null engine");

@@ -55,6 +55,7 @@ struct OpDesc {
   uint8_t m[VSGM_MAX_QV];
   int8_t other;                 // COMPUTE_COUNT: computed vertex to count against (-1: none)
   uint8_t other_op;             // relation candidate(u) OP candidate(other)
+  uint16_t merge_ratio;         // intersect by merging when list lengths are within this ratio (0: always gallop)
 };
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -294,7 +295,7 @@ __global__ void k_copy_marked(Frame f, OpDesc d, const uint64_t* __restrict__ of
 // Warp intersection of the backward lists of one path.  emit(ok, c) is called by
 // every lane once per step; the lanes with ok hold candidates, in increasing
 // order across lanes and steps.
-//  - merge: when the second-shortest restricted list is at most kMergeRatio
+//  - merge: when the second-shortest restricted list is at most merge_ratio
 //    times the shortest, both are streamed 32 at a time (coalesced) and each lane
 //    finds its element of the shortest list in the other's window by a
 //    register binary search over shuffles;
@@ -302,10 +303,13 @@ __global__ void k_copy_marked(Frame f, OpDesc d, const uint64_t* __restrict__ of
 //    forward in the longer lists.
 // Any remaining lists (three or more backward neighbours) are galloped.
 // ---------------------------------------------------------------------------
-constexpr uint64_t kMergeRatio = 4;
-
-template <int NB, typename Emit>
-__device__ __forceinline__ void intersect_warp(const Window& w, const Lists& L, const uint32_t* __restrict__ ci, Emit&& emit) {
+// kCount: the caller only counts, so emit may be called by single lanes at any
+// time (no ballot inside); long similar-length lists then use the lane-partitioned
+// merge: the shorter list is cut into 32 equal chunks, each lane finds its start in
+// the other list by binary search and merges its chunk sequentially (32
+// independent streams per warp instead of one latency-bound window step).
+template <int NB, bool kCount = false, typename Emit>
+__device__ __forceinline__ void intersect_warp(const Window& w, const Lists& L, const uint32_t* __restrict__ ci, uint32_t merge_ratio, Emit&& emit) {
   const unsigned lane = lane_id();
   uint64_t pos[NB];
 #pragma unroll
@@ -321,7 +325,37 @@ __device__ __forceinline__ void intersect_warp(const Window& w, const Lists& L, 
       jb = j;
     }
   const uint64_t alen = L.pe - L.ps;
-  if (NB >= 2 && alen >= 64 && blen <= kMergeRatio * alen) {
+  if (kCount && NB >= 2 && alen >= 256 && blen <= (uint64_t)merge_ratio * alen) {
+    const uint64_t chunk = (alen + kWarp - 1) / kWarp;
+    uint64_t i = L.ps + lane * chunk;
+    const uint64_t i1 = (i + chunk < L.pe) ? i + chunk : L.pe;
+    if (i < i1) {
+      uint32_t x = __ldg(ci + i);
+      uint64_t j = lower_bound(ci, bs, be, x);
+      while (i < i1 && j < be) {
+        const uint32_t y = __ldg(ci + j);
+        if (x < y) {
+          if (++i < i1) x = __ldg(ci + i);
+        } else if (y < x) {
+          j++;
+        } else {
+          bool ok = ne_ok(w, x);
+#pragma unroll
+          for (int q = 0; q < NB; q++) {
+            if (q == L.pivot || q == jb || !ok) continue;
+            uint64_t r = gallop(ci, pos[q], L.e[q], x);
+            pos[q] = r;
+            ok = (r < L.e[q]) && (__ldg(ci + r) == x);
+          }
+          if (ok) emit(true, x);
+          j++;
+          if (++i < i1) x = __ldg(ci + i);
+        }
+      }
+    }
+    return;
+  }
+  if (NB >= 2 && alen >= 64 && blen <= (uint64_t)merge_ratio * alen) {
     uint64_t ia = L.ps, ib = bs;
     while (ia < L.pe && ib < be) {
       const uint32_t nA = (uint32_t)(L.pe - ia < (uint64_t)kWarp ? L.pe - ia : (uint64_t)kWarp);
@@ -387,7 +421,7 @@ __global__ void k_compute_write(Frame f, OpDesc d, const uint64_t* __restrict__ 
     restrict_lists(d, mine, w, rp, ci, &L);
     uint32_t* out = pool + off[p];
     uint32_t written = 0;
-    intersect_warp<NB>(w, L, ci, [&](bool ok, uint32_t c) {
+    intersect_warp<NB>(w, L, ci, d.merge_ratio, [&](bool ok, uint32_t c) {
       unsigned mask = __ballot_sync(kFull, ok);
       if (ok) out[written + __popc(mask & ((1u << lane) - 1))] = c;
       written += __popc(mask);
@@ -432,7 +466,7 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
       oset = set_of(f, d.other, p);
       on = __ldg(f.clen[d.other] + p);
     }
-    intersect_warp<NB>(w, L, ci, [&](bool ok, uint32_t c) {
+    intersect_warp<NB, true>(w, L, ci, d.merge_ratio, [&](bool ok, uint32_t c) {
       if (ok) acc += kOther ? count_vs(oset, on, &ocur, c, d.other_op) : 1ull;
     });
   }
@@ -542,7 +576,7 @@ __global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const 
           ni += __popc(mask);
         }
       } else {
-        intersect_warp<NK>(w, L, ci, [&](bool ok, uint32_t c) {
+        intersect_warp<NK>(w, L, ci, d.merge_ratio, [&](bool ok, uint32_t c) {
           unsigned mask = __ballot_sync(kFull, ok);
           if (ok) I[ni + __popc(mask & ((1u << lane) - 1))] = c;
           ni += __popc(mask);
@@ -666,7 +700,7 @@ __global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const 
           }
         if (lane == 0) acc_bytes += 4ull * (Lc.pe - Lc.ps) + 16ull * (NK + 1);
         uint64_t ocur = 0;
-        intersect_warp<NK + 1>(wc, Lc, ci, [&](bool ok, uint32_t x) {
+        intersect_warp<NK + 1, true>(wc, Lc, ci, d.merge_ratio, [&](bool ok, uint32_t x) {
           if (ok) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
         });
       }
@@ -720,6 +754,11 @@ __global__ void k_expand(Frame in, Expand x, const uint64_t* __restrict__ off, u
         out.clen[x.cu[i]][c] = __ldg(in.clen[x.cu[i]] + p);
       }
   }
+}
+
+// every stride-th root (sampled runs of the autotuner)
+__global__ void k_stride_copy(const uint32_t* __restrict__ in, uint64_t n_out, uint64_t stride, uint32_t* __restrict__ out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_out; i += (uint64_t)gridDim.x * blockDim.x) out[i] = in[i * stride];
 }
 
 // ---------------------------------------------------------------------------
