@@ -212,6 +212,24 @@ void* vsgm_engine_stream(vsgm_engine* e);
 
 const char* vsgm_engine_error(vsgm_engine* e);
 
+/* Allocation-free counting.  This entry point has no counterpart in the
+ * reference.  It is for callers that may not allocate device memory - code that
+ * runs under a pool or allocator owning all of the process's device memory, or that
+ * must have a fixed footprint known before it runs: it counts one plan over one
+ * view already in device memory (d_row_ptrs[V+1], d_cols, d_sources[n_sources]) and
+ * writes the exact count to *count (host memory), using the same persistent kernel
+ * as vsgm_run_batched but with all of its working buffers inside one 48 MiB
+ * file-scope device array, which every GPU that loads this library holds until the
+ * process exits.  It calls no cudaMalloc or cudaFree.  The first call on a device
+ * looks up the array's device address (make that first call before any stream
+ * capture).  Limit: plan ops x the view's maximum degree <= 24,383; larger views
+ * are rejected with VSGM_EINVAL and a message.  The array is shared by every call on
+ * the device and keeps the last call's contents (each call clears what it needs):
+ * calls that overlap on the GPU race, so serialise them.  stream may be NULL (the
+ * legacy default stream); the call returns after the stream is synchronised. */
+int vsgm_count_noalloc(int device, const vsgm_plan* plan, uint64_t V, const uint64_t* d_row_ptrs, const uint32_t* d_cols, const uint32_t* d_sources,
+                       uint64_t n_sources, void* stream, uint64_t* count);
+
 /* ~PipelineExecutor (src/executor/pipeline_executor.h:48-54). */
 int vsgm_destroy(vsgm_engine* e);
 

@@ -1,0 +1,56 @@
+"""Allocation-free counting (vsgm_count_noalloc) against the batched engine.
+
+Some callers cannot allocate device memory: their process hands all of it to a
+pool or allocator it does not control, or the code path must have a footprint
+fixed before it runs.  vsgm_count_noalloc serves them from a fixed file-scope
+device array.  Its exact counts must equal vsgm_run_batched's on the same
+device-resident view, on two calls in a row (the second call finds the first
+call's leftovers in the shared array).  Kept in its own file, collected last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(vs, plan, V, rp, ci, src, n):
+    out = C.c_uint64()
+    rc = vs.capi.lib().vsgm_count_noalloc(0, C.byref(plan), V, C.c_void_p(rp.data_ptr()), C.c_void_p(ci.data_ptr()),
+                                          C.c_void_p(src.data_ptr()), n, None, C.byref(out))
+    return rc, out.value
+
+
+def test_noalloc_counts_equal_batched_on_two_calls(vs):
+    import torch
+
+    g = vs.gen_rmat(9, 8, seed=21)
+    plans = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(4), vs.plan_pattern(13)]
+    with vs.Engine(g.V, plans) as e:
+        vid = e.add_view(g)
+        want = [row[0] for row in e.run_batched([vid])]
+    rp = torch.from_numpy(g.row_ptrs.view(np.int64)).cuda()
+    ci = torch.from_numpy(g.cols.view(np.int32)).cuda()
+    src = torch.arange(g.V, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        for p, w in zip(plans, want):
+            rc, got = _noalloc(vs, p, g.V, rp, ci, src, g.V)
+            assert rc == 0, vs.capi.lib().vsgm_engine_error(None)
+            assert got == w
+
+
+def test_noalloc_rejects_views_beyond_its_limit(vs):
+    import torch
+
+    n = 30000  # a star: one vertex of degree 30000
+    rp = np.zeros(n + 2, np.uint64)
+    rp[1] = n
+    rp[2:] = n + np.arange(1, n + 1)
+    cols = np.concatenate([np.arange(1, n + 1), np.zeros(n)]).astype(np.uint32)
+    d_rp = torch.from_numpy(rp.view(np.int64)).cuda()
+    d_ci = torch.from_numpy(cols.view(np.int32)).cuda()
+    d_src = torch.arange(n + 1, dtype=torch.int32, device="cuda")
+    rc, _ = _noalloc(vs, vs.plan_clique(4), n + 1, d_rp, d_ci, d_src, n + 1)
+    assert rc != 0
+    assert b"allocation-free" in vs.capi.lib().vsgm_engine_error(None)

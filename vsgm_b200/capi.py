@@ -145,6 +145,7 @@ _SIGS = {
     "vsgm_engine_stream": (C.c_void_p, [C.c_void_p]),
     "vsgm_engine_error": (C.c_char_p, [C.c_void_p]),
     "vsgm_destroy": (C.c_int, [C.c_void_p]),
+    "vsgm_count_noalloc": (C.c_int, [C.c_int, _P(Plan), C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, _u64p]),
     "vsgm_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64, _P(C.c_void_p)]),
     "vsgm_mlp_num_params": (C.c_uint64, [C.c_void_p]),
     "vsgm_mlp_get_params": (C.c_int, [C.c_void_p, _P(C.c_float)]),

@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -1045,3 +1047,128 @@ int vsgm_destroy(vsgm_engine* e) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- allocation-free entry point
+//
+// vsgm_count_noalloc counts one plan over one view that is already in device
+// memory without allocating anything: it runs the persistent depth-first kernel
+// (k_dfs, the kernel behind vsgm_run_batched) with every buffer it needs - task
+// list, counters and the per-warp candidate scratch - carved out of one
+// file-scope device array of fixed size.  It is meant for callers that must not
+// call cudaMalloc: code running inside a memory pool or allocator that owns all
+// device memory of the process, code paths whose memory footprint has to be known
+// before they run, and embeddings whose host side cannot manage device
+// allocations.  Every GPU that loads this library holds the array until the
+// process exits.
+namespace {
+
+constexpr size_t kNoAllocBytes = 48ull << 20;  // the whole static scratch
+constexpr unsigned kNoAllocBlocks = 64;         // 64 blocks x 8 warps
+constexpr uint64_t kNoAllocWarps = (uint64_t)kNoAllocBlocks * kDfsWarps;
+constexpr uint64_t kNoAllocMaxTasks = 16384;
+// layout: [0, 256) counters | [256, 1280) plan + view | tasks | per-warp scratch
+constexpr size_t kNoAllocHeader = 256;
+constexpr size_t kNoAllocDescOff = 256;
+constexpr size_t kNoAllocTaskOff = 1280;
+constexpr size_t kNoAllocScratchOff = (kNoAllocTaskOff + kNoAllocMaxTasks * sizeof(DfsTask) + 255) & ~(size_t)255;
+constexpr uint64_t kNoAllocWarpU32 = (kNoAllocBytes - kNoAllocScratchOff) / (kNoAllocWarps * sizeof(uint32_t));
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// device address of g_noalloc_scratch per device (the host-side symbol is not a
+// device address; cudaGetSymbolAddress gives the real one)
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[128] = {};
+
+struct NoAllocCounters {
+  unsigned long long head;
+  unsigned long long count;
+  unsigned long long max_degree;
+  unsigned int status;
+};
+
+__global__ void k_noalloc_max_degree(const uint64_t* __restrict__ rp, uint64_t V, NoAllocCounters* c) {
+  unsigned long long m = 0;
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long d = rp[v + 1] - rp[v];
+    if (d > m) m = d;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long y = __shfl_down_sync(kFull, m, o);
+    if (y > m) m = y;
+  }
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(&c->max_degree, m);
+}
+
+__global__ void k_noalloc_tasks(DfsTask* tasks, uint64_t n_tasks, uint64_t n_sources, uint64_t chunk) {
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_tasks; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r0 = t * chunk;
+    tasks[t] = DfsTask{0u, 0u, r0, r0 + chunk < n_sources ? r0 + chunk : n_sources};
+  }
+}
+
+int noalloc_fail(const std::string& msg) { return engine_fail(nullptr, VSGM_EINVAL, msg); }
+
+}  // namespace
+
+extern "C" int vsgm_count_noalloc(int device, const vsgm_plan* plan, uint64_t V, const uint64_t* d_row_ptrs, const uint32_t* d_cols,
+                                  const uint32_t* d_sources, uint64_t n_sources, void* stream, uint64_t* count) {
+  if (!plan || !count || !d_row_ptrs || (n_sources && !d_sources)) return noalloc_fail("null argument");
+  if (V == 0 || V >= 0xffffffffull) return noalloc_fail("vertex count must be 1 .. 2^32-2");
+  if (plan->n_vertices < 2 || plan->n_vertices > VSGM_MAX_QV || plan->n_ops < 2 || plan->n_ops > VSGM_MAX_OPS || plan->op_type[0] != VSGM_MATERIALIZE)
+    return noalloc_fail("malformed plan");
+  if (device < 0 || device >= 128) return noalloc_fail("device index out of range");
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = guarded(nullptr, [&] {
+    CK(cudaSetDevice(device));
+    unsigned char* base = nullptr;
+    {
+      std::lock_guard<std::mutex> lock(g_noalloc_mu);
+      if (!g_noalloc_ptr[device]) {
+        // once per device, with that device current
+        CK(cudaGetSymbolAddress((void**)&g_noalloc_ptr[device], g_noalloc_scratch));
+      }
+      base = g_noalloc_ptr[device];
+    }
+    NoAllocCounters* ctr = (NoAllocCounters*)base;
+    DfsPlan* d_plan = (DfsPlan*)(base + kNoAllocDescOff);
+    DfsView* d_view = (DfsView*)(base + kNoAllocDescOff + sizeof(DfsPlan));
+    DfsTask* d_tasks = (DfsTask*)(base + kNoAllocTaskOff);
+    uint32_t* scratch = (uint32_t*)(base + kNoAllocScratchOff);
+    // the array keeps the previous call's contents: clear the counters
+    CK(cudaMemsetAsync(ctr, 0, sizeof(NoAllocCounters), s));
+    k_noalloc_max_degree<<<256, 256, 0, s>>>(d_row_ptrs, V, ctr);
+    CK(cudaGetLastError());
+    NoAllocCounters h{};
+    CK(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const uint64_t cap = std::max<uint64_t>(1, h.max_degree);
+    const uint32_t levels = plan->n_ops;
+    if ((uint64_t)levels * cap > kNoAllocWarpU32)
+      throw std::invalid_argument("view too large for the allocation-free path: plan ops x maximum degree = " + std::to_string(levels * cap) +
+                                  ", limit " + std::to_string(kNoAllocWarpU32));
+    if (n_sources == 0) {
+      *count = 0;
+      return;
+    }
+    const DfsPlan hp = vsgm_engine::to_dfs(*plan);
+    const DfsView hv{d_row_ptrs, d_cols, d_sources};
+    CK(cudaMemcpyAsync(d_plan, &hp, sizeof(hp), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_view, &hv, sizeof(hv), cudaMemcpyHostToDevice, s));
+    const uint64_t chunk = std::max<uint64_t>(16, (n_sources + kNoAllocMaxTasks - 1) / kNoAllocMaxTasks);
+    const uint64_t n_tasks = (n_sources + chunk - 1) / chunk;
+    k_noalloc_tasks<<<64, 256, 0, s>>>(d_tasks, n_tasks, n_sources, chunk);
+    CK(cudaGetLastError());
+    k_dfs<<<kNoAllocBlocks, kDfsWarps * kWarp, 0, s>>>(d_plan, d_view, d_tasks, n_tasks, &ctr->head, scratch, cap, levels, 1u, &ctr->count,
+                                                       &ctr->status, nullptr, 0, nullptr);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(&h, ctr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (h.status) throw std::invalid_argument("a candidate set did not fit in the allocation-free scratch");
+    *count = h.count;
+  });
+  if (prev >= 0) cudaSetDevice(prev);
+  return rc;
+}
