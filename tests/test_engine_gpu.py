@@ -244,10 +244,12 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
     with vs.Engine(g.V, plans) as e:
         e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
         for ratio in (0, 1, 2, 64):
-            e.set_option("merge_ratio", ratio)
-            e.reset_counts()
-            e.match()
-            assert e.counts() == want, ratio
+            for lane in (0, 1):
+                e.set_option("merge_ratio", ratio)
+                e.set_option("lane_merge", lane)
+                e.reset_counts()
+                e.match()
+                assert e.counts() == want, (ratio, lane)
         report = autotune(e, len(plans), stride=4)
         assert [r["plan"] for r in report] == list(range(len(plans)))
         e.match()

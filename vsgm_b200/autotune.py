@@ -1,7 +1,7 @@
 """Autotuner for the engine's per-plan knobs (intersection variant and tail fusion).
 
 For every plan it times each candidate setting of (fuse_tail, merge_ratio,
-stage_cap) on a strided sample of the view's roots (engine option root_stride)
+lane_merge, stage_cap) on a strided sample of the view's roots (engine option root_stride)
 and keeps the fastest; the choice is written back as per-plan options.  Counts
 never depend on these knobs, so tuning on a sample is safe; the sample only has
 to rank the settings.
@@ -11,7 +11,8 @@ import time
 
 CANDIDATES = {
     "fuse_tail": (1, 0),
-    "merge_ratio": (0, 2, 4, 16),
+    "merge_ratio": (0, 4, 16),
+    "lane_merge": (0, 1),
     "stage_cap": (1536, 384),
 }
 
@@ -22,6 +23,8 @@ def _settings(space):
         cfg = dict(zip(keys, vals))
         if not cfg["fuse_tail"] and cfg["stage_cap"] != space["stage_cap"][0]:
             continue  # the stage only matters for the fused tail
+        if cfg.get("lane_merge") and not cfg["merge_ratio"]:
+            continue  # no merge, nothing to partition
         yield cfg
 
 

@@ -108,6 +108,7 @@ struct vsgm_engine {
     bool fuse_tail = true;           // fused MATERIALIZE + COMPUTE_COUNT
     uint32_t stage_cap = kStageCap;  // shared-memory stage of the fused tail, in u32
     uint32_t merge_ratio = 4;        // merge vs gallop threshold of the warp intersection
+    bool lane_merge = false;         // counting kernels: lane-partitioned merge
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -228,6 +229,7 @@ struct vsgm_engine {
     d.u = p.op_vertex[i];
     d.other = -1;
     d.merge_ratio = (uint16_t)cur.merge_ratio;
+    d.lane_merge = cur.lane_merge ? 1 : 0;
     const vsgm_vgroup& mg = p.materialized[i];
     d.nm = mg.count;
     int slot[VSGM_MAX_QV];
@@ -932,6 +934,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   if (n == "stage_cap") {
     if (value < 0 || value > kStageCap) return engine_fail(e, VSGM_EINVAL, "stage_cap must be 0.." + std::to_string(kStageCap));
     for (int k = lo; k < hi; k++) e->knobs[k].stage_cap = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "lane_merge") {
+    for (int k = lo; k < hi; k++) e->knobs[k].lane_merge = value != 0;
     return VSGM_OK;
   }
   if (n == "merge_ratio") {

@@ -56,6 +56,7 @@ struct OpDesc {
   int8_t other;                 // COMPUTE_COUNT: computed vertex to count against (-1: none)
   uint8_t other_op;             // relation candidate(u) OP candidate(other)
   uint16_t merge_ratio;         // intersect by merging when list lengths are within this ratio (0: always gallop)
+  uint8_t lane_merge;           // counting kernels: lane-partitioned instead of windowed merge
 };
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
@@ -309,7 +310,8 @@ __global__ void k_copy_marked(Frame f, OpDesc d, const uint64_t* __restrict__ of
 // the other list by binary search and merges its chunk sequentially (32
 // independent streams per warp instead of one latency-bound window step).
 template <int NB, bool kCount = false, typename Emit>
-__device__ __forceinline__ void intersect_warp(const Window& w, const Lists& L, const uint32_t* __restrict__ ci, uint32_t merge_ratio, Emit&& emit) {
+__device__ __forceinline__ void intersect_warp(const Window& w, const Lists& L, const uint32_t* __restrict__ ci, uint32_t merge_ratio, Emit&& emit,
+                                               bool lane_merge = false) {
   const unsigned lane = lane_id();
   uint64_t pos[NB];
 #pragma unroll
@@ -325,7 +327,7 @@ __device__ __forceinline__ void intersect_warp(const Window& w, const Lists& L, 
       jb = j;
     }
   const uint64_t alen = L.pe - L.ps;
-  if (kCount && NB >= 2 && alen >= 256 && blen <= (uint64_t)merge_ratio * alen) {
+  if (kCount && lane_merge && NB >= 2 && alen >= 256 && blen <= (uint64_t)merge_ratio * alen) {
     const uint64_t chunk = (alen + kWarp - 1) / kWarp;
     uint64_t i = L.ps + lane * chunk;
     const uint64_t i1 = (i + chunk < L.pe) ? i + chunk : L.pe;
@@ -466,9 +468,11 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
       oset = set_of(f, d.other, p);
       on = __ldg(f.clen[d.other] + p);
     }
-    intersect_warp<NB, true>(w, L, ci, d.merge_ratio, [&](bool ok, uint32_t c) {
-      if (ok) acc += kOther ? count_vs(oset, on, &ocur, c, d.other_op) : 1ull;
-    });
+    intersect_warp<NB, true>(
+        w, L, ci, d.merge_ratio, [&](bool ok, uint32_t c) {
+          if (ok) acc += kOther ? count_vs(oset, on, &ocur, c, d.other_op) : 1ull;
+        },
+        d.lane_merge);
   }
   for (int o = 16; o > 0; o >>= 1) {
     acc += __shfl_down_sync(kFull, acc, o);
@@ -700,9 +704,11 @@ __global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const 
           }
         if (lane == 0) acc_bytes += 4ull * (Lc.pe - Lc.ps) + 16ull * (NK + 1);
         uint64_t ocur = 0;
-        intersect_warp<NK + 1, true>(wc, Lc, ci, d.merge_ratio, [&](bool ok, uint32_t x) {
-          if (ok) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
-        });
+        intersect_warp<NK + 1, true>(
+            wc, Lc, ci, d.merge_ratio, [&](bool ok, uint32_t x) {
+              if (ok) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
+            },
+            d.lane_merge);
       }
     }
   }
