@@ -81,6 +81,7 @@ def test_stats_match_oracle_paths(vs, orc, graphs):
     for p in [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(3)]:
         total, paths = orc.op_paths(p, g)
         with vs.Engine(g.V, [p]) as e:
+            e.set_option("c4_aggregate", 0)  # the op sequence itself
             e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
             e.match()
             assert e.counts() == [total]
@@ -259,3 +260,22 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
         e.reset_counts()
         e.match()
         assert e.counts()[1] == orc.count(plans[1], g, np.arange(0, g.V, 3, dtype=np.uint32))
+
+
+def test_four_cycle_aggregation_equals_plan(vs, orc, graphs):
+    """Wedge aggregation (each 4-cycle at its largest vertex) gives the plan's total, on any labels."""
+    p = vs.plan_pattern(1)
+    hub, _ = vs.degree_relabel(_hub_graph(vs))
+    for g in (graphs["rmat7"], graphs["rmat8"], graphs["chunglu"], vs.degree_relabel(graphs["rmat8"])[0],
+              vs.degree_relabel(graphs["rmat8"], ascending=False)[0], hub, cycle_graph(vs, 4), complete_graph(vs, 6)):
+        want = orc.count(p, g)
+        for agg in (1, 0):
+            with vs.Engine(g.V, [p]) as e:
+                e.set_option("c4_aggregate", agg)
+                e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+                e.match()
+                assert e.counts() == [want], agg
+    # views: per-view attribution differs, totals do not
+    g = graphs["rmat8"]
+    bins = (np.arange(g.V) % 3).astype(np.int32)
+    assert vs.count_graph(g, [p], views=vs.sources_of_bins(bins, 3)) == [orc.count(p, g)]

@@ -10,6 +10,7 @@ import itertools
 import time
 
 CANDIDATES = {
+    "c4_aggregate": (1, 0),
     "fuse_tail": (1, 0),
     "merge_ratio": (0, 4, 16),
     "lane_merge": (0, 1),
@@ -25,6 +26,9 @@ def _settings(space):
             continue  # the stage only matters for the fused tail
         if cfg.get("lane_merge") and not cfg["merge_ratio"]:
             continue  # no merge, nothing to partition
+        if cfg.get("c4_aggregate") and (cfg["fuse_tail"] != space["fuse_tail"][0] or cfg["merge_ratio"] != space["merge_ratio"][0]
+                                        or cfg.get("lane_merge") or cfg["stage_cap"] != space["stage_cap"][0]):
+            continue  # the other knobs do not matter when a 4-cycle is aggregated
         yield cfg
 
 

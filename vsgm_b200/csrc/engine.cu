@@ -109,6 +109,7 @@ struct vsgm_engine {
     uint32_t stage_cap = kStageCap;  // shared-memory stage of the fused tail, in u32
     uint32_t merge_ratio = 4;        // merge vs gallop threshold of the warp intersection
     bool lane_merge = false;         // counting kernels: lane-partitioned merge
+    bool c4_aggregate = true;        // 4-cycle plans: wedge aggregation instead of the op sequence
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -602,6 +603,36 @@ struct vsgm_engine {
     CK(cudaGetLastError());
   }
 
+  // the pattern is a 4-cycle: four vertices, four edges, every vertex of degree two
+  static bool is_four_cycle(const vsgm_plan& p) {
+    if (p.n_vertices != 4 || p.n_edges != 4) return false;
+    for (int i = 0; i < 4; i++)
+      if (__builtin_popcount(p.adj[i]) != 2) return false;
+    return true;
+  }
+
+  // 4-cycles rooted at the given sources, by wedge aggregation (k_c4_aggregate);
+  // each cycle is attributed to its largest vertex, the plan attributes it to its
+  // smallest: totals over all sources are the same
+  void c4_aggregate(const uint32_t* roots, uint64_t n) {
+    const int last = (int)plan->n_ops - 1;
+    Mark m(arena);
+    const uint64_t per_block = 2ull * V * sizeof(uint32_t);
+    uint64_t blocks = std::min<uint64_t>((uint64_t)sms * 4, (arena.avail() > (1u << 20) ? arena.avail() - (1u << 20) : 0) / per_block);
+    if (blocks == 0) throw OutOfMemory{"HBM budget exhausted (4-cycle counters)"};
+    blocks = std::min<uint64_t>(blocks, std::max<uint64_t>(1, n));
+    uint32_t* L = arena.take_n<uint32_t>(blocks * V, "4-cycle counters");
+    uint32_t* touched = arena.take_n<uint32_t>(blocks * V, "4-cycle touched ids");
+    unsigned long long* head = arena.take_n<unsigned long long>(1, "4-cycle queue head");
+    begin_op();
+    CK(cudaMemsetAsync(L, 0, blocks * V * sizeof(uint32_t), stream));
+    CK(cudaMemsetAsync(head, 0, sizeof(unsigned long long), stream));
+    k_c4_aggregate<<<(unsigned)blocks, 256, 0, stream>>>(d_rp, d_ci, roots, n, V, L, touched, head, d_total);
+    CK(cudaGetLastError());
+    end_op(last, 1);
+    st->op_paths[last] += n;
+  }
+
   static DfsPlan to_dfs(const vsgm_plan& p) {
     DfsPlan d;
     std::memset(&d, 0, sizeof(d));
@@ -749,7 +780,11 @@ struct vsgm_engine {
     }
     st->op_paths[0] += f.P;
     st->op_outputs[0] += f.P;
-    process(1, f);
+    if (cur.c4_aggregate && is_four_cycle(*plan)) {
+      c4_aggregate(f.col[plan->op_vertex[0]], f.P);
+    } else {
+      process(1, f);
+    }
     if (profiling) {
       // the CC kernel accumulated algorithmic bytes
       uint64_t b = read_u64((const uint64_t*)d_bytes);
@@ -934,6 +969,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   if (n == "stage_cap") {
     if (value < 0 || value > kStageCap) return engine_fail(e, VSGM_EINVAL, "stage_cap must be 0.." + std::to_string(kStageCap));
     for (int k = lo; k < hi; k++) e->knobs[k].stage_cap = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "c4_aggregate") {
+    for (int k = lo; k < hi; k++) e->knobs[k].c4_aggregate = value != 0;
     return VSGM_OK;
   }
   if (n == "lane_merge") {

@@ -762,6 +762,67 @@ __global__ void k_expand(Frame in, Expand x, const uint64_t* __restrict__ off, u
   }
 }
 
+// ---------------------------------------------------------------------------
+// 4-cycle count by wedge aggregation.  Every 4-cycle is counted once, at its
+// largest vertex u: for each neighbour v < u and each w in N(v) with w < u,
+// L[w] counts the wedges u-v-w; the cycles closed at u are sum C(L[w], 2)
+// (pairs of distinct v through the same opposite vertex w).  Work is bounded by
+// sum over edges of the smaller degree when ids ascend with degree, instead of
+// intersecting the two wedge ends' lists for every wedge (the plan's COMPUTE_COUNT).
+// One block per root; each block owns a dense counter array over the ids and a
+// list of the ids it touched, used to sum and reset.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ roots,
+                                                      uint64_t n_roots, uint64_t V, uint32_t* __restrict__ L_all, uint32_t* __restrict__ touched_all,
+                                                      unsigned long long* __restrict__ head, unsigned long long* __restrict__ total) {
+  __shared__ unsigned long long s_root;
+  __shared__ unsigned int s_touched;
+  __shared__ unsigned long long s_sum[8];
+  uint32_t* L = L_all + (uint64_t)blockIdx.x * V;
+  uint32_t* touched = touched_all + (uint64_t)blockIdx.x * V;
+  const unsigned lane = lane_id(), warp = threadIdx.x / kWarp, nwarps = blockDim.x / kWarp;
+  unsigned long long acc = 0;
+  while (true) {
+    if (threadIdx.x == 0) {
+      s_root = atomicAdd(head, 1ull);
+      s_touched = 0;
+    }
+    __syncthreads();
+    const unsigned long long r = s_root;
+    if (r >= n_roots) break;
+    const uint32_t u = __ldg(roots + r);
+    const uint64_t ua = __ldg(rp + u), uz = __ldg(rp + u + 1);
+    // wedges: warp per neighbour v < u, lanes over N(v) below u
+    for (uint64_t k = ua + warp; k < uz; k += nwarps) {
+      const uint32_t v = __ldg(ci + k);
+      if (v >= u) break;  // rows are sorted
+      const uint64_t va = __ldg(rp + v), vz = __ldg(rp + v + 1);
+      for (uint64_t j = va + lane; j < vz; j += kWarp) {
+        const uint32_t w = __ldg(ci + j);
+        if (w >= u) break;
+        if (atomicAdd(L + w, 1u) == 0u) touched[atomicAdd(&s_touched, 1u)] = w;
+      }
+    }
+    __syncthreads();
+    const unsigned n = s_touched;
+    for (unsigned i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t w = touched[i];
+      const unsigned long long c = L[w];
+      acc += c * (c - 1) / 2;
+      L[w] = 0;
+    }
+    __syncthreads();
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if (lane == 0) s_sum[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (unsigned i = 0; i < nwarps; i++) t += s_sum[i];
+    if (t) atomicAdd(total, t);
+  }
+}
+
 // every stride-th root (sampled runs of the autotuner)
 __global__ void k_stride_copy(const uint32_t* __restrict__ in, uint64_t n_out, uint64_t stride, uint32_t* __restrict__ out) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_out; i += (uint64_t)gridDim.x * blockDim.x) out[i] = in[i * stride];
