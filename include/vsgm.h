@@ -201,12 +201,15 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   rooted at each cycle's largest vertex (sum over opposite vertices of
  *   C(wedges, 2)) instead of the plan's op sequence; totals are identical, per-view
  *   counts are attributed to the largest instead of the smallest vertex;
+ *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT
+ *   of a vertex with the same backward lists and conditions (the diamond's tail)
+ *   counts the pairs of one intersection instead of intersecting twice;
  *   "lane_merge" (default 0): counting kernels merge two such lists with each lane
  *   walking its own chunk instead of 32-element warp windows;
  *   "root_stride" (engine-wide, default 1): match only every k-th source of the view
  *   (the autotuner's samples; counts are then those of the sample);
  *   "only_plan" (engine-wide, default -1): vsgm_match runs only this plan.
- * fuse_tail, stage_cap, merge_ratio, lane_merge and c4_aggregate never change a total count. */
+ * None of the knobs changes a total count. */
 int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t value);
 int vsgm_set_option(vsgm_engine* e, const char* name, int64_t value);
 

@@ -279,3 +279,15 @@ def test_four_cycle_aggregation_equals_plan(vs, orc, graphs):
     g = graphs["rmat8"]
     bins = (np.arange(g.V) % 3).astype(np.int32)
     assert vs.count_graph(g, [p], views=vs.sources_of_bins(bins, 3)) == [orc.count(p, g)]
+
+
+@pytest.mark.parametrize("reuse", [0, 1])
+def test_set_reuse_pairs(vs, orc, graphs, reuse):
+    """Diamond-like tails (count against an identical candidate set): pairs of one set."""
+    g = graphs["chunglu"]
+    plans = [vs.plan_pattern(2)] + [p for _, p in all_plans(vs) if _.startswith("km")]
+    with vs.Engine(g.V, plans) as e:
+        e.set_option("set_reuse", reuse)
+        e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+        e.match()
+        assert e.counts() == [orc.count(p, g) for p in plans]

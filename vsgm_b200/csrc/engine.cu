@@ -110,6 +110,7 @@ struct vsgm_engine {
     uint32_t merge_ratio = 4;        // merge vs gallop threshold of the warp intersection
     bool lane_merge = false;         // counting kernels: lane-partitioned merge
     bool c4_aggregate = true;        // 4-cycle plans: wedge aggregation instead of the op sequence
+    bool set_reuse = true;           // COMPUTE o + COMPUTE_COUNT w over the same set: count pairs of one intersection
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -393,9 +394,53 @@ struct vsgm_engine {
     }
   }
 
+  // COMPUTE(o) followed by the final COMPUTE_COUNT(w) counted against o, with the
+  // same backward lists and the same conditions on the same materialised vertices:
+  // both candidate sets are one set S, and the count per path is the number of
+  // pairs of S the condition between w and o admits
+  int same_set_pairs(int i, int o) const {
+    const vsgm_plan& p = *plan;
+    if (!cur.set_reuse || i + 1 != (int)p.n_ops - 1 || p.op_type[i + 1] != VSGM_COMPUTE_COUNT) return 0;
+    const int w = p.op_vertex[i + 1];
+    const vsgm_vgroup& cu = p.computed_unmat[i + 1];
+    if (cu.count != 1 || cu.v[0] != o) return 0;
+    if (p.materialized[i].count != p.materialized[i + 1].count) return 0;
+    const vsgm_vgroup &bw = p.backward[w], &bo = p.backward[o];
+    if (bw.count != bo.count) return 0;
+    for (int k = 0; k < bw.count; k++)
+      if (bw.v[k] != bo.v[k]) return 0;
+    const vsgm_conds &cw = p.compute_cond[w], &co = p.compute_cond[o];
+    if (cw.count != co.count) return 0;
+    for (int k = 0; k < cw.count; k++)
+      if (cw.v[k] != co.v[k] || cw.op[k] != co.op[k]) return 0;
+    const uint8_t rel = p.order[w][o];
+    return (rel == VSGM_LESS_THAN || rel == VSGM_LARGER_THAN) ? 1 : (rel == VSGM_NON_EQUAL ? 2 : 0);
+  }
+
   void op_compute(int i, const Frame& f, int u) {
     const vsgm_plan& p = *plan;
     OpDesc d = make_desc(i, p.compute_cond[u]);
+    if (const int mode = same_set_pairs(i, u)) {
+      begin_op();
+      switch (d.nb) {
+#define VSGM_PAIRS(NB)                                                                                              \
+  case NB:                                                                                                          \
+    k_compute_count<NB, false, false><<<grid_warps(f.P), 256, 0, stream>>>(f, d, d_rp, d_ci, d_total, d_bytes, mode); \
+    break;
+        VSGM_PAIRS(1)
+        VSGM_PAIRS(2)
+        VSGM_PAIRS(3)
+        VSGM_PAIRS(4)
+        VSGM_PAIRS(5)
+        VSGM_PAIRS(6)
+#undef VSGM_PAIRS
+        default: throw OutOfMemory{"pattern vertex with no backward neighbour"};
+      }
+      CK(cudaGetLastError());
+      end_op(i + 1, 1);
+      st->op_paths[i + 1] += f.P;
+      return;
+    }
     if (d.nb == 1) {
       narrow_then(i, f, d, true, u, [&](const Frame& g) { process(i + 1, g); });
       return;
@@ -969,6 +1014,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   if (n == "stage_cap") {
     if (value < 0 || value > kStageCap) return engine_fail(e, VSGM_EINVAL, "stage_cap must be 0.." + std::to_string(kStageCap));
     for (int k = lo; k < hi; k++) e->knobs[k].stage_cap = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "set_reuse") {
+    for (int k = lo; k < hi; k++) e->knobs[k].set_reuse = value != 0;
     return VSGM_OK;
   }
   if (n == "c4_aggregate") {

@@ -449,9 +449,12 @@ __device__ __forceinline__ uint64_t count_vs(const uint32_t* __restrict__ a, uin
   return n - (eq ? 1 : 0);
 }
 
+// pair_mode (same candidate set counted against itself, see the engine's
+// set-reuse rule): 0 = plain count, 1 = C(n, 2) per path, 2 = n (n - 1) per path
 template <int NB, bool kOther, bool kBytes>
 __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                                                       unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
+                                                       unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes,
+                                                       int pair_mode = 0) {
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
   const unsigned lane = lane_id();
   unsigned long long acc = 0, acc_bytes = 0;
@@ -467,6 +470,14 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
     if (kOther) {
       oset = set_of(f, d.other, p);
       on = __ldg(f.clen[d.other] + p);
+    }
+    if (pair_mode) {
+      unsigned long long n = 0;
+      intersect_warp<NB, true>(
+          w, L, ci, d.merge_ratio, [&](bool ok, uint32_t) { n += ok ? 1ull : 0ull; }, d.lane_merge);
+      for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(kFull, n, o);
+      if (lane == 0 && n > 1) acc += pair_mode == 1 ? n * (n - 1) / 2 : n * (n - 1);
+      continue;
     }
     intersect_warp<NB, true>(
         w, L, ci, d.merge_ratio, [&](bool ok, uint32_t c) {
