@@ -122,6 +122,22 @@ int vsgm_transfer_view(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t*
  * copy; the caller keeps it alive until the next transfer or destroy). */
 int vsgm_bind_view_device(vsgm_engine* e, const uint64_t* d_row_ptrs, const uint32_t* d_cols, uint64_t n_cols, const uint32_t* d_sources, uint64_t n_sources);
 
+/* Keep the whole graph resident on the engine's device (row_ptrs[V+1], cols)
+ * so that views can be built there: replaces the host producers of
+ * src/app/pattern_matching_pipeline.cu:117-150 (one LoadViewBin per bin). */
+int vsgm_upload_graph(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n_cols);
+
+/* ViewBin::Materialize (src/view/view_bin.h:66-142) on the device from the
+ * uploaded graph: the halo of the sources (degree >= root_degree, all when 0)
+ * within hop-1 steps gets its full rows; the result becomes the current view
+ * with exactly these sources, byte-identical to vsgm_view_materialize. */
+int vsgm_materialize_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_sources, int hop, uint64_t root_degree);
+
+/* Copy the current view back to the host (row_ptrs[V+1], cols[cols_cap]);
+ * VSGM_ENOMEM with *n_cols set when cols_cap is too small.  No reference
+ * counterpart (inspection of a device-built view). */
+int vsgm_read_view(vsgm_engine* e, uint64_t* row_ptrs, uint32_t* cols, uint64_t cols_cap, uint64_t* n_cols);
+
 /* PipelineExecutor::Match (src/executor/pipeline_executor.h:83-109): run every
  * plan over every source of the current view and add to the per-plan totals. */
 int vsgm_match(vsgm_engine* e);

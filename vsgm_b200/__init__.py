@@ -211,6 +211,27 @@ class Engine:
         capi.check(_L().vsgm_bind_view_device(self.h, C.c_void_p(d_row_ptrs), C.c_void_p(d_cols), n_cols,
                                               C.c_void_p(d_sources), n_sources), self.h)
 
+    def upload_graph(self, g):
+        """Keep the whole graph on the device; views are then built there by materialize_view."""
+        self._graph = g
+        capi.check(_L().vsgm_upload_graph(self.h, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32), g.E), self.h)
+
+    def materialize_view(self, sources, hop, root_degree=0):
+        """ViewBin::Materialize on the device: the sources' halo becomes the current view."""
+        sources = np.ascontiguousarray(sources, dtype=np.uint32)
+        capi.check(_L().vsgm_materialize_view(self.h, capi.ptr(sources, C.c_uint32), len(sources), int(hop), int(root_degree)), self.h)
+
+    def read_view(self):
+        """The current view copied back to the host, as a Graph."""
+        rp = np.zeros(self.V + 1, np.uint64)
+        n = C.c_uint64()
+        rc = _L().vsgm_read_view(self.h, capi.ptr(rp, C.c_uint64), None, 0, C.byref(n))
+        if rc not in (0, capi.ENOMEM):
+            capi.check(rc, self.h)
+        ci = np.zeros(max(n.value, 1), np.uint32)
+        capi.check(_L().vsgm_read_view(self.h, capi.ptr(rp, C.c_uint64), capi.ptr(ci, C.c_uint32), n.value, C.byref(n)), self.h)
+        return Graph(rp, ci[:n.value])
+
     def match(self):
         capi.check(_L().vsgm_match(self.h), self.h)
 

@@ -131,6 +131,9 @@ _SIGS = {
     "vsgm_create": (C.c_int, [C.c_int, C.c_uint64, _P(Plan), C.c_int, C.c_uint64, C.c_uint64, _P(C.c_void_p)]),
     "vsgm_transfer_view": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64, _u32p, C.c_uint64]),
     "vsgm_bind_view_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64]),
+    "vsgm_upload_graph": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64]),
+    "vsgm_materialize_view": (C.c_int, [C.c_void_p, _u32p, C.c_uint64, C.c_int, C.c_uint64]),
+    "vsgm_read_view": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64, _u64p]),
     "vsgm_match": (C.c_int, [C.c_void_p]),
     "vsgm_get_counts": (C.c_int, [C.c_void_p, _u64p]),
     "vsgm_reset_counts": (C.c_int, [C.c_void_p]),
@@ -182,6 +185,9 @@ def lib(path=None):
 
 class VsgmError(RuntimeError):
     pass
+
+
+ENOMEM = -4  # VSGM_ENOMEM
 
 
 def check(rc, engine=None):

@@ -94,6 +94,10 @@ struct vsgm_engine {
   uint64_t* own_rp = nullptr;
   uint32_t* own_ci = nullptr;
   uint32_t* own_src = nullptr;
+  // full graph resident for device-side view materialisation (vsgm_upload_graph)
+  uint64_t* g_rp = nullptr;
+  uint32_t* g_ci = nullptr;
+  uint64_t g_cols = 0;
 
   Arena arena;
   unsigned long long* d_counts = nullptr;  // [n_plans]
@@ -957,6 +961,96 @@ int vsgm_bind_view_device(vsgm_engine* e, const uint64_t* d_row_ptrs, const uint
   return VSGM_OK;
 }
 
+int vsgm_upload_graph(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n_cols) {
+  if (!e || !row_ptrs || (n_cols && !cols)) return engine_fail(e, VSGM_EINVAL, "null graph argument");
+  if (row_ptrs[e->V] != n_cols) return engine_fail(e, VSGM_EINVAL, "row_ptrs[V] != n_cols");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    if (e->g_rp) CK(cudaFree(e->g_rp));
+    if (e->g_ci) CK(cudaFree(e->g_ci));
+    e->g_rp = nullptr;
+    e->g_ci = nullptr;
+    CK(cudaMalloc(&e->g_rp, sizeof(uint64_t) * (e->V + 1)));
+    CK(cudaMalloc(&e->g_ci, sizeof(uint32_t) * std::max<uint64_t>(n_cols, 1)));
+    CK(cudaMemcpyAsync(e->g_rp, row_ptrs, sizeof(uint64_t) * (e->V + 1), cudaMemcpyHostToDevice, e->stream));
+    if (n_cols) CK(cudaMemcpyAsync(e->g_ci, cols, sizeof(uint32_t) * n_cols, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    e->g_cols = n_cols;
+  });
+}
+
+int vsgm_materialize_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_sources, int hop, uint64_t root_degree) {
+  if (!e || (n_sources && !sources)) return engine_fail(e, VSGM_EINVAL, "null view argument");
+  if (!e->g_rp) return engine_fail(e, VSGM_EINVAL, "no graph uploaded");
+  if (hop < 1) return engine_fail(e, VSGM_EINVAL, "hop must be >= 1");
+  for (uint64_t i = 0; i < n_sources; i++)
+    if (sources[i] >= e->V) return engine_fail(e, VSGM_EINVAL, "source id out of range");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    const uint64_t V = e->V;
+    if (n_sources > e->src_cap) {
+      if (e->own_src) CK(cudaFree(e->own_src));
+      e->own_src = nullptr;
+      CK(cudaMalloc(&e->own_src, sizeof(uint32_t) * n_sources));
+      e->src_cap = n_sources;
+    }
+    if (n_sources) CK(cudaMemcpyAsync(e->own_src, sources, sizeof(uint32_t) * n_sources, cudaMemcpyHostToDevice, e->stream));
+    Mark m(e->arena);
+    e->arena.top = 0;
+    // membership flags: one byte per vertex, whole words so the flag update is a word atomic
+    uint8_t* flags = (uint8_t*)e->arena.take_n<uint32_t>((V + 3) / 4 + 1, "view flags");
+    uint32_t* cur = e->arena.take_n<uint32_t>(std::max<uint64_t>(V, 1), "view frontier");
+    uint32_t* nxt = e->arena.take_n<uint32_t>(std::max<uint64_t>(V, 1), "view frontier");
+    unsigned long long* cnt = e->arena.take_n<unsigned long long>(2, "view counters");
+    uint64_t* len = e->arena.take_n<uint64_t>(V + 1, "view row lengths");
+    CK(cudaMemsetAsync(flags, 0, sizeof(uint32_t) * ((V + 3) / 4 + 1), e->stream));
+    CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * 2, e->stream));
+    k_halo_seed2<<<e->grid_threads(n_sources), 256, 0, e->stream>>>(e->g_rp, e->own_src, n_sources, root_degree, flags, cur, cnt);
+    CK(cudaGetLastError());
+    uint64_t n_cur = e->read_u64((const uint64_t*)cnt);
+    for (int layer = 1; layer < hop && n_cur; layer++) {
+      CK(cudaMemsetAsync(cnt + 1, 0, sizeof(unsigned long long), e->stream));
+      k_halo_layer<<<e->grid_warps(n_cur), 256, 0, e->stream>>>(e->g_rp, e->g_ci, V, cur, n_cur, flags, nxt, cnt + 1);
+      CK(cudaGetLastError());
+      n_cur = e->read_u64((const uint64_t*)(cnt + 1));
+      std::swap(cur, nxt);
+    }
+    k_halo_lengths<<<e->grid_threads(V), 256, 0, e->stream>>>(e->g_rp, V, flags, len);
+    CK(cudaGetLastError());
+    e->scan(len, false, V, e->own_rp);
+    const uint64_t total = e->read_u64(e->own_rp + V);
+    if (total > e->cols_cap) {
+      if (e->own_ci) CK(cudaFree(e->own_ci));
+      e->own_ci = nullptr;
+      CK(cudaMalloc(&e->own_ci, sizeof(uint32_t) * std::max<uint64_t>(total, 1)));
+      e->cols_cap = total;
+    }
+    k_halo_copy<<<e->grid_warps(V), 256, 0, e->stream>>>(e->g_rp, e->g_ci, V, flags, e->own_rp, e->own_ci);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(e->stream));
+    e->d_rp = e->own_rp;
+    e->d_ci = e->own_ci;
+    e->d_src = e->own_src;
+    e->n_cols = total;
+    e->n_src = n_sources;
+    e->have_view = true;
+  });
+}
+
+int vsgm_read_view(vsgm_engine* e, uint64_t* row_ptrs, uint32_t* cols, uint64_t cols_cap, uint64_t* n_cols) {
+  if (!e || !row_ptrs || !n_cols) return engine_fail(e, VSGM_EINVAL, "null argument");
+  if (!e->have_view) return engine_fail(e, VSGM_EINVAL, "no view transferred");
+  *n_cols = e->n_cols;
+  if (e->n_cols > cols_cap || (e->n_cols && !cols)) return engine_fail(e, VSGM_ENOMEM, "view has more adjacency entries than cols_cap");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    CK(cudaMemcpyAsync(row_ptrs, e->d_rp, sizeof(uint64_t) * (e->V + 1), cudaMemcpyDeviceToHost, e->stream));
+    if (e->n_cols) CK(cudaMemcpyAsync(cols, e->d_ci, sizeof(uint32_t) * e->n_cols, cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+  });
+}
+
 int vsgm_match(vsgm_engine* e) {
   if (!e) return engine_fail(nullptr, VSGM_EINVAL, "null engine");
   if (!e->have_view) return engine_fail(e, VSGM_EINVAL, "no view transferred");
@@ -1127,6 +1221,8 @@ int vsgm_destroy(vsgm_engine* e) {
   cudaFree(e->own_rp);
   cudaFree(e->own_ci);
   cudaFree(e->own_src);
+  cudaFree(e->g_rp);
+  cudaFree(e->g_ci);
   for (auto& r : e->rviews) {
     cudaFree(r.rp);
     cudaFree(r.ci);

@@ -834,6 +834,59 @@ __global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict
   }
 }
 
+// ---------------------------------------------------------------------------
+// View materialisation on the device (ViewBin::Materialize, src/view/view_bin.h:49-142):
+// sources of degree >= root_degree start the halo, each further layer adds the
+// neighbours of the previous one, then every vertex in the halo gets its full row.
+// ---------------------------------------------------------------------------
+// flags are one byte per vertex, set with a byte-wise compare-and-swap on the word
+__device__ __forceinline__ bool set_flag(uint8_t* flags, uint32_t v) {
+  unsigned int* word = (unsigned int*)(flags + (v & ~3u));
+  const unsigned int bit = 0xffu << ((v & 3u) * 8);
+  unsigned int old = atomicOr(word, bit);
+  return (old & bit) == 0;
+}
+
+__global__ void k_halo_seed2(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ src, uint64_t n, uint64_t root_degree,
+                             uint8_t* __restrict__ in_view, uint32_t* __restrict__ frontier, unsigned long long* __restrict__ n_frontier) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t s = src[i];
+    if (root_degree && rp[s + 1] - rp[s] < root_degree) continue;
+    if (set_flag(in_view, s)) frontier[atomicAdd(n_frontier, 1ull)] = s;
+  }
+}
+
+// one warp per frontier vertex: unseen neighbours join the view and the next frontier
+__global__ void k_halo_layer(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t V, const uint32_t* __restrict__ frontier,
+                             uint64_t n, uint8_t* __restrict__ in_view, uint32_t* __restrict__ next, unsigned long long* __restrict__ n_next) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < n; i += warps) {
+    const uint32_t x = frontier[i];
+    for (uint64_t j = rp[x] + lane; j < rp[x + 1]; j += kWarp) {
+      const uint32_t y = ci[j];
+      if (y < V && set_flag(in_view, y)) next[atomicAdd(n_next, 1ull)] = y;  // ids >= V (a corrupt file) are skipped
+    }
+  }
+}
+
+__global__ void k_halo_lengths(const uint64_t* __restrict__ rp, uint64_t V, const uint8_t* __restrict__ in_view, uint64_t* __restrict__ len) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x)
+    len[v] = in_view[v] ? rp[v + 1] - rp[v] : 0;
+}
+
+// one warp per vertex of the view: copy its row
+__global__ void k_halo_copy(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t V, const uint8_t* __restrict__ in_view,
+                            const uint64_t* __restrict__ out_rp, uint32_t* __restrict__ out_ci) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; v < V; v += warps) {
+    if (!in_view[v]) continue;
+    const uint64_t a = rp[v], n = rp[v + 1] - a, o = out_rp[v];
+    for (uint64_t j = lane; j < n; j += kWarp) out_ci[o + j] = ci[a + j];
+  }
+}
+
 // every stride-th root (sampled runs of the autotuner)
 __global__ void k_stride_copy(const uint32_t* __restrict__ in, uint64_t n_out, uint64_t stride, uint32_t* __restrict__ out) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_out; i += (uint64_t)gridDim.x * blockDim.x) out[i] = in[i * stride];

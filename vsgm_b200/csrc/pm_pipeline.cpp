@@ -2,11 +2,14 @@
 // (src/app/pattern_matching_pipeline.cu:27-201), over the vsgm C ABI.
 //
 //   pm_pipeline -f <graph.bin> [-m GB] [-p P | -kc k | -km k] [-t threads] [-qs queue]
-//               [-pn producers] [-cn consumers] [-dm 0|1] [-df 0|1] [-dr 0|1] [-ds 0|1] [-dst n]
+//               [-pn producers] [-cn consumers] [-dm 0|1] [-df 0|1] [-dr 0|1] [-ds 0|1] [-dst n] [-gv 0|1]
 //
-// Producers materialise view bins (k-hop halos) on the host into a bounded
-// queue of host buffers; one consumer per GPU uploads each view, matches every
-// plan and accumulates exact counts.  Prints "total count for query i: N" and
+// With -gv 1 (default) every consumer keeps the whole graph on its GPU and
+// builds each view bin's k-hop halo there (vsgm_materialize_view); producers
+// only hand out bin ids.  With -gv 0 producers materialise the halos on the
+// host into a bounded queue of host buffers, as the reference does, and each
+// consumer uploads them.  Either way one consumer per GPU matches every plan
+// and accumulates exact counts.  Prints "total count for query i: N" and
 // "finish total time, elapsed_time=Xms" like the reference.
 #include <sys/stat.h>
 #include <sys/time.h>
@@ -30,7 +33,7 @@ namespace {
 struct Args {
   std::string file = "./data/com-friendster.ungraph.txt.bin";
   double mem = 10;
-  int pattern = 1, kc = 0, km = 0, threads = 1, qs = 1, pn = 1, cn = 1, dm = 1, df = 1, dr = 0, ds = 0, dst = 1;
+  int pattern = 1, kc = 0, km = 0, threads = 1, qs = 1, pn = 1, cn = 1, dm = 1, df = 1, dr = 0, ds = 0, dst = 1, gv = 1;
 };
 
 // CommandLine's linear scan (src/common/command_line.h:32-86)
@@ -109,6 +112,7 @@ int main(int argc, char** argv) {
   if (auto v = opt(argc, argv, "-dr")) a.dr = std::atoi(v);
   if (auto v = opt(argc, argv, "-ds")) a.ds = std::atoi(v);
   if (auto v = opt(argc, argv, "-dst")) a.dst = std::atoi(v);
+  if (auto v = opt(argc, argv, "-gv")) a.gv = std::atoi(v);
   if (a.qs < a.cn || a.pn < 1 || a.cn < 1) {
     std::fprintf(stderr, "error: need -qs >= -cn >= 1 and -pn >= 1\n");
     return 1;
@@ -190,6 +194,10 @@ int main(int argc, char** argv) {
         View* v = new View();
         v->id = (int)id;
         v->sources = pool[id];
+        if (a.gv) {  // the consumer builds the halo on its GPU
+          q.push(v);
+          continue;
+        }
         v->row_ptrs.resize(V + 1);
         v->cols.resize(cap);
         if (vsgm_view_materialize(V, rp, ci, v->sources.data(), v->sources.size(), hop, root_degree, a.threads, v->row_ptrs.data(), v->cols.data(),
@@ -211,8 +219,16 @@ int main(int argc, char** argv) {
         while (View* v = q.pop()) delete v;  // keep producers moving
         return;
       }
+      if (a.gv && vsgm_upload_graph(e, rp, ci, E)) {
+        std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(e));
+        failed = 1;
+        while (View* v = q.pop()) delete v;
+        vsgm_destroy(e);
+        return;
+      }
       while (View* v = q.pop()) {
-        int rc = vsgm_transfer_view(e, v->row_ptrs.data(), v->cols.data(), v->n_cols, v->sources.data(), v->sources.size());
+        int rc = a.gv ? vsgm_materialize_view(e, v->sources.data(), v->sources.size(), hop, root_degree)
+                      : vsgm_transfer_view(e, v->row_ptrs.data(), v->cols.data(), v->n_cols, v->sources.data(), v->sources.size());
         delete v;  // the host buffers are free once the transfer returns
         if (!rc && a.dm) rc = vsgm_match(e);
         if (rc) {
