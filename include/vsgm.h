@@ -133,6 +133,13 @@ int vsgm_upload_graph(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* 
  * with exactly these sources, byte-identical to vsgm_view_materialize. */
 int vsgm_materialize_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_sources, int hop, uint64_t root_degree);
 
+/* The uploaded graph itself becomes the current view, with these sources as
+ * roots: every row is present, so no halo is built.  Counts equal those over
+ * the sources' k-hop halo (a match rooted at a source reads only rows inside
+ * its halo).  No reference counterpart: the reference never holds the whole
+ * graph on the GPU. */
+int vsgm_graph_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_sources);
+
 /* Copy the current view back to the host (row_ptrs[V+1], cols[cols_cap]);
  * VSGM_ENOMEM with *n_cols set when cols_cap is too small.  No reference
  * counterpart (inspection of a device-built view). */

@@ -77,6 +77,13 @@ def test_device_views_count_like_host_views(vs, orc, graphs):
             e.match()
         got = e.counts()
     assert got == [orc.count(p, g) for p in plans]
+    # the resident graph as the view of every bin: same totals, no halo built
+    with vs.Engine(g.V, plans) as e:
+        e.upload_graph(g)
+        for src in bins:
+            e.graph_view(src)
+            e.match()
+        assert e.counts() == got
     for G in (complete_graph(vs, 8), cycle_graph(vs, 10)):
         with vs.Engine(G.V, plans) as e:
             e.upload_graph(G)
@@ -86,7 +93,8 @@ def test_device_views_count_like_host_views(vs, orc, graphs):
 
 
 def test_pm_pipeline_device_views(vs, orc, graphs, tmp_path):
-    """The CLI gives the same counts with host-built (-gv 0) and device-built (-gv 1) views."""
+    """The CLI gives the same counts with host-built halos (-gv 0), device-built halos
+    (-gv 1) and the resident whole graph as every bin's view (-gv 2)."""
     from vsgm_b200 import build
 
     g = graphs["rmat8"]
@@ -95,7 +103,7 @@ def test_pm_pipeline_device_views(vs, orc, graphs, tmp_path):
     bins = (np.arange(g.V) * 7 % 5).astype(np.int32)
     vs.write_vbmap(str(path) + ".2.hop.vbmap", bins, 5)
     want = orc.count(vs.plan_pattern(2), g)
-    for gv in ("0", "1"):
+    for gv in ("0", "1", "2"):
         out = subprocess.run([build.DRIVER, "-f", str(path), "-m", "1", "-p", "2", "-pn", "2", "-cn", "1", "-gv", gv],
                              capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr

@@ -221,6 +221,12 @@ class Engine:
         sources = np.ascontiguousarray(sources, dtype=np.uint32)
         capi.check(_L().vsgm_materialize_view(self.h, capi.ptr(sources, C.c_uint32), len(sources), int(hop), int(root_degree)), self.h)
 
+    def graph_view(self, sources):
+        """The uploaded graph itself is the view; only the roots change."""
+        sources = np.ascontiguousarray(sources, dtype=np.uint32)
+        self._keep_src = sources
+        capi.check(_L().vsgm_graph_view(self.h, capi.ptr(sources, C.c_uint32), len(sources)), self.h)
+
     def read_view(self):
         """The current view copied back to the host, as a Graph."""
         rp = np.zeros(self.V + 1, np.uint64)

@@ -133,6 +133,7 @@ _SIGS = {
     "vsgm_bind_view_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64]),
     "vsgm_upload_graph": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64]),
     "vsgm_materialize_view": (C.c_int, [C.c_void_p, _u32p, C.c_uint64, C.c_int, C.c_uint64]),
+    "vsgm_graph_view": (C.c_int, [C.c_void_p, _u32p, C.c_uint64]),
     "vsgm_read_view": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64, _u64p]),
     "vsgm_match": (C.c_int, [C.c_void_p]),
     "vsgm_get_counts": (C.c_int, [C.c_void_p, _u64p]),

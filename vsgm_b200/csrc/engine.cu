@@ -1038,6 +1038,30 @@ int vsgm_materialize_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_so
   });
 }
 
+int vsgm_graph_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_sources) {
+  if (!e || (n_sources && !sources)) return engine_fail(e, VSGM_EINVAL, "null view argument");
+  if (!e->g_rp) return engine_fail(e, VSGM_EINVAL, "no graph uploaded");
+  for (uint64_t i = 0; i < n_sources; i++)
+    if (sources[i] >= e->V) return engine_fail(e, VSGM_EINVAL, "source id out of range");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    if (n_sources > e->src_cap) {
+      if (e->own_src) CK(cudaFree(e->own_src));
+      e->own_src = nullptr;
+      CK(cudaMalloc(&e->own_src, sizeof(uint32_t) * n_sources));
+      e->src_cap = n_sources;
+    }
+    if (n_sources) CK(cudaMemcpyAsync(e->own_src, sources, sizeof(uint32_t) * n_sources, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    e->d_rp = e->g_rp;
+    e->d_ci = e->g_ci;
+    e->d_src = e->own_src;
+    e->n_cols = e->g_cols;
+    e->n_src = n_sources;
+    e->have_view = true;
+  });
+}
+
 int vsgm_read_view(vsgm_engine* e, uint64_t* row_ptrs, uint32_t* cols, uint64_t cols_cap, uint64_t* n_cols) {
   if (!e || !row_ptrs || !n_cols) return engine_fail(e, VSGM_EINVAL, "null argument");
   if (!e->have_view) return engine_fail(e, VSGM_EINVAL, "no view transferred");

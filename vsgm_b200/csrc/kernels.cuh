@@ -839,7 +839,8 @@ __global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict
 // sources of degree >= root_degree start the halo, each further layer adds the
 // neighbours of the previous one, then every vertex in the halo gets its full row.
 // ---------------------------------------------------------------------------
-// flags are one byte per vertex, set with a byte-wise compare-and-swap on the word
+// flags are one byte per vertex; a word-wide atomicOr of the byte's mask sets one and
+// tells the one thread that set it first
 __device__ __forceinline__ bool set_flag(uint8_t* flags, uint32_t v) {
   unsigned int* word = (unsigned int*)(flags + (v & ~3u));
   const unsigned int bit = 0xffu << ((v & 3u) * 8);

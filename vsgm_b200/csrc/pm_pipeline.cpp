@@ -2,14 +2,16 @@
 // (src/app/pattern_matching_pipeline.cu:27-201), over the vsgm C ABI.
 //
 //   pm_pipeline -f <graph.bin> [-m GB] [-p P | -kc k | -km k] [-t threads] [-qs queue]
-//               [-pn producers] [-cn consumers] [-dm 0|1] [-df 0|1] [-dr 0|1] [-ds 0|1] [-dst n] [-gv 0|1]
+//               [-pn producers] [-cn consumers] [-dm 0|1] [-df 0|1] [-dr 0|1] [-ds 0|1] [-dst n] [-gv 0|1|2]
 //
-// With -gv 1 (default) every consumer keeps the whole graph on its GPU and
-// builds each view bin's k-hop halo there (vsgm_materialize_view); producers
-// only hand out bin ids.  With -gv 0 producers materialise the halos on the
-// host into a bounded queue of host buffers, as the reference does, and each
-// consumer uploads them.  Either way one consumer per GPU matches every plan
-// and accumulates exact counts.  Prints "total count for query i: N" and
+// With -gv 2 (default) every consumer keeps the whole graph on its GPU and
+// matches each view bin's sources over it directly (vsgm_graph_view, no halo
+// needed); with -gv 1 it builds each bin's k-hop halo there
+// (vsgm_materialize_view).  In both, producers only hand out bin ids.  With
+// -gv 0 producers materialise the halos on the host into a bounded queue of
+// host buffers, as the reference does, and each consumer uploads them.
+// Either way one consumer per GPU matches every plan and accumulates exact
+// counts.  Prints "total count for query i: N" and
 // "finish total time, elapsed_time=Xms" like the reference.
 #include <sys/stat.h>
 #include <sys/time.h>
@@ -33,7 +35,7 @@ namespace {
 struct Args {
   std::string file = "./data/com-friendster.ungraph.txt.bin";
   double mem = 10;
-  int pattern = 1, kc = 0, km = 0, threads = 1, qs = 1, pn = 1, cn = 1, dm = 1, df = 1, dr = 0, ds = 0, dst = 1, gv = 1;
+  int pattern = 1, kc = 0, km = 0, threads = 1, qs = 1, pn = 1, cn = 1, dm = 1, df = 1, dr = 0, ds = 0, dst = 1, gv = 2;
 };
 
 // CommandLine's linear scan (src/common/command_line.h:32-86)
@@ -227,8 +229,9 @@ int main(int argc, char** argv) {
         return;
       }
       while (View* v = q.pop()) {
-        int rc = a.gv ? vsgm_materialize_view(e, v->sources.data(), v->sources.size(), hop, root_degree)
-                      : vsgm_transfer_view(e, v->row_ptrs.data(), v->cols.data(), v->n_cols, v->sources.data(), v->sources.size());
+        int rc = a.gv == 2 ? vsgm_graph_view(e, v->sources.data(), v->sources.size())
+                 : a.gv  ? vsgm_materialize_view(e, v->sources.data(), v->sources.size(), hop, root_degree)
+                         : vsgm_transfer_view(e, v->row_ptrs.data(), v->cols.data(), v->n_cols, v->sources.data(), v->sources.size());
         delete v;  // the host buffers are free once the transfer returns
         if (!rc && a.dm) rc = vsgm_match(e);
         if (rc) {
