@@ -8,6 +8,10 @@ every source (what view_packing produces for this graph under a 40 GB budget).
 A step is one match of all three queries over the resident view.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--scale S] [--queries kc4,p1,p2] [--option knob=value ...]
+
+(--scale / --queries / --option select smaller or single-query cases for
+profiling; the default is the workload above.)
 
 value   = sum of the exact counts / device time per step (inputs resident in HBM)
 e2e     = the same through the C ABI from pinned host buffers: view upload +
@@ -46,12 +50,31 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def make_workload(vs, scale=22, edge_factor=16, seed=2, relabel="asc"):
+def parse_queries(text):
+    """"kc4,p1,p2" -> reference flags ["-kc 4", "-p 1", "-p 2"]."""
+    flags = []
+    for q in text.split(","):
+        q = q.strip()
+        if q.startswith("kc"):
+            flags.append(f"-kc {int(q[2:])}")
+        elif q.startswith("p"):
+            flags.append(f"-p {int(q[1:])}")
+        else:
+            raise SystemExit(f"unknown query {q!r} (kcK or pN)")
+    return flags
+
+
+def plan_of(vs, flag):
+    kind, k = flag.split()
+    return vs.plan_clique(int(k)) if kind == "-kc" else vs.plan_pattern(int(k))
+
+
+def make_workload(vs, scale=22, edge_factor=16, seed=2, relabel="asc", queries=None):
     t = time.time()
     g = vs.gen_rmat(scale, edge_factor, 0.57, 0.19, 0.19, seed=seed)
     if relabel != "none":
         g, _ = vs.degree_relabel(g, ascending=(relabel == "asc"))
-    plans = [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2)]
+    plans = [plan_of(vs, f) for f in (queries or WORKLOAD["queries"])]
     log(f"graph V={g.V} E={g.E} generated+relabelled in {time.time() - t:.1f}s; plans:", [p.describe() for p in plans])
     return g, plans
 
@@ -128,7 +151,7 @@ def run_reference(args):
         return 0
     import vsgm_b200 as vs
     vs.capi.lib()
-    g, plans = make_workload(vs, scale=args.scale, relabel=args.relabel)
+    g, plans = make_workload(vs, scale=args.scale, relabel=args.relabel, queries=args.query_flags)
     threads = os.cpu_count() or 1
     per_step = []
     for s in range(args.warmup + args.steps):
@@ -137,7 +160,7 @@ def run_reference(args):
             per_step.append((rate, cnt, secs, nroots))
     rate = float(np.mean([r[0] for r in per_step]))
     secs = float(np.mean([r[2] for r in per_step]))
-    sample = (f"{per_step[-1][3]} random roots of {g.V} per step (time-boxed {args.ref_seconds}s, split over the 3 queries); "
+    sample = (f"{per_step[-1][3]} random roots of {g.V} per step (time-boxed {args.ref_seconds}s, summed over the {len(plans)} queries); "
               f"matches/s = sampled matches / sampled seconds")
     out = {"impl": "reference", "metric": "matches/s", "value": rate, "unit": "matches/s", "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
@@ -160,7 +183,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--relabel", default="asc", choices=["asc", "desc", "none"])
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--queries", default="kc4,p1,p2", help="comma list of kcK / pN (default: the workload's three)")
+    ap.add_argument("--option", action="append", default=[], help="engine knob name=value (vsgm_set_option), repeatable")
     args = ap.parse_args()
+    args.query_flags = parse_queries(args.queries)
+    if args.query_flags != WORKLOAD["queries"] or args.scale != 22:
+        WORKLOAD["workload"] = f"rmat{args.scale}_ef16_seed2_" + "_".join(q.strip() for q in args.queries.split(","))
+        WORKLOAD["queries"] = args.query_flags
+        WORKLOAD["graph"] = WORKLOAD["graph"].replace("scale 22", f"scale {args.scale}")
     if args.impl == "reference":
         return run_reference(args)
 
@@ -176,12 +206,15 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    g, plans = make_workload(vs, scale=args.scale, relabel=args.relabel)
+    g, plans = make_workload(vs, scale=args.scale, relabel=args.relabel, queries=args.query_flags)
     # roots of this rank: a strided share of the vertices (one view per rank)
     from vsgm_b200.shard import allreduce_counts, roots_of_rank
     roots = roots_of_rank(g.V, rank, world)
     eng = vs.Engine(g.V, plans, device=local)
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
+    for kv in args.option:
+        name, val = kv.split("=")
+        eng.set_option(name, int(val))
 
     # ---------------- device-resident timing (value)
     eng.transfer_view(g, roots)
@@ -269,7 +302,7 @@ def main():
         threads = os.cpu_count() or 1
         rate, cnt, secs, nroots = cpu_sample_rate(g, plans, args.cpu_seconds, threads)
         cpu = {"value": rate, "unit": "matches/s", "cores": threads, "kind": "port",
-               "sample": f"{nroots} random roots (time-boxed {args.cpu_seconds}s over the 3 queries), matches/s = sampled matches / seconds"}
+               "sample": f"{nroots} random roots (time-boxed {args.cpu_seconds}s over the {len(plans)} queries), matches/s = sampled matches / seconds"}
 
     if rank == 0:
         out = {"metric": "matches/s", "value": value, "unit": "matches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
