@@ -236,6 +236,33 @@ def test_batched_level_paths_and_step_budget(vs, orc, graphs):
         assert all(int(cnt2[i][0]) <= int(cnt[i][0]) for i in range(len(plans)))
 
 
+@pytest.mark.parametrize("fuse", [0, 1])
+def test_batched_heavy_roots_and_fused_tail(vs, orc, graphs, fuse):
+    """The persistent run splits a hub root's candidates over several warps and fuses
+    the last MATERIALIZE with the final count: counts and per-op partial matches
+    still equal the oracle's."""
+    plans = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2), vs.plan_pattern(3),
+             vs.plan_pattern(4), vs.plan_pattern(13)]
+    ctr = 0
+    for _ in range(6):
+        n, bits, ctr = vs.random_pattern(seed=5, counter=ctr, n_min=4, n_max=5)
+        plans.append(vs.plan_query_bits(n, bits))
+    hub = _hub_graph(vs, leaves=1200, chords=1500)
+    views = [vs.degree_relabel(hub, ascending=True)[0], vs.degree_relabel(hub, ascending=False)[0], graphs["rmat7"]]
+    V = max(g.V for g in views)
+    with vs.Engine(V, plans) as e:
+        e.set_option("fuse_tail", fuse)
+        ids = [e.add_view(g) for g in views]
+        cnt, lvl, ovf = e.run_batched_ex(ids)
+        assert e.batch_stats().tasks > len(plans) * len(views)
+        assert not ovf.any()
+    for i, p in enumerate(plans):
+        for v, g in enumerate(views):
+            total, paths = orc.op_paths(p, g)
+            assert int(cnt[i][v]) == total, (p.describe(), v)
+            assert [int(x) for x in lvl[i][v][:p.n_ops]] == paths, (p.describe(), v)
+
+
 def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
     """Every intersection variant / fusion setting gives the same counts; the autotuner picks one."""
     from vsgm_b200.autotune import autotune

@@ -29,9 +29,24 @@ struct DfsOp {
   uint8_t cu0, cu1, cu_op;
 };
 
+// The last MATERIALIZE(u) fused with the final COMPUTE_COUNT(w) (same rule as the
+// level-wise engine's fused tail): the lists and conditions of w that do not
+// involve u are intersected once per parent, then every child c of u counts its
+// share of that set in N(c), one child per lane.
+struct DfsFused {
+  uint8_t on, lvl;     // lvl: the MATERIALIZE's op index
+  uint8_t has_cond_u;  // condition  candidate(w)  cond_u_op  c
+  uint8_t cond_u_op;
+  int8_t other;        // computed vertex counted against (-1 none)
+  uint8_t other_op;
+  DfsOp known;         // nb/b: backward lists of w without u; nc/cop/cv: conditions of w not on u
+};
+
 struct DfsPlan {
   uint32_t n_ops;
   uint32_t root;
+  uint32_t split_lvl;  // first MATERIALIZE after the root (n_ops if none): where a root's work can be split
+  DfsFused fz;
   DfsOp op[VSGM_MAX_OPS];
 };
 
@@ -44,6 +59,9 @@ struct DfsView {
 struct DfsTask {
   uint32_t plan, view;
   uint64_t r0, r1;  // source index range within the view
+  // c1 != 0: a share of one heavy root (r1 == r0 + 1): only the candidates
+  // [c0, c1) of the plan's split level are expanded, so several warps share it
+  uint32_t c0, c1;
 };
 
 constexpr int kDfsWarps = 8;  // warps per block
@@ -181,6 +199,114 @@ __device__ __forceinline__ bool dfs_has_ne(const uint32_t* a, uint32_t n, const 
   return hit;
 }
 
+// Fused tail of one parent (DfsFused): children are cs[k0, n) minus the values in
+// skip[]; I is a scratch buffer of at least the largest degree.  Returns the
+// matches; *n_children = children expanded (what the unfused walk would enter).
+__device__ __forceinline__ unsigned long long dfs_fused(const DfsFused& fz, const uint32_t* M, const uint32_t* cs, uint32_t k0, uint32_t n,
+                                                        const uint32_t* skip, const uint32_t* oset, uint32_t on, const uint64_t* __restrict__ rp,
+                                                        const uint32_t* __restrict__ ci, uint32_t* I, uint64_t* n_children) {
+  const unsigned lane = lane_id();
+  unsigned long long acc = 0;
+  uint32_t kids = 0;
+  for (uint32_t k = k0 + lane; k < n; k += kWarp) {
+    const uint32_t c = cs[k];
+    bool sk = false;
+#pragma unroll
+    for (int i = 0; i < VSGM_MAX_QV; i++) sk |= (c == skip[i]);
+    kids += sk ? 0u : 1u;
+  }
+  for (int o = 16; o > 0; o >>= 1) kids += __shfl_xor_sync(kFull, kids, o);
+  *n_children = kids;
+  if (kids == 0) return 0;
+  Window w;
+  dfs_window(fz.known, M, &w);  // conditions not involving u
+  Window ws = w;
+  if (fz.has_cond_u && fz.cond_u_op == VSGM_LARGER_THAN) window_add(&ws, VSGM_LARGER_THAN, cs[k0], 0);
+  if (fz.has_cond_u && fz.cond_u_op == VSGM_LESS_THAN) window_add(&ws, VSGM_LESS_THAN, cs[n - 1], 0);
+  Lists L;
+  dfs_lists(fz.known, M, ws, rp, ci, &L);
+  uint32_t ni = 0;
+  if (fz.known.nb == 1) {
+    ni = dfs_filter_copy(ci + L.ps, (uint32_t)(L.pe - L.ps), w, I);
+  } else {
+    dfs_intersect(fz.known, w, L, ci, [&](bool ok, uint32_t c) {
+      unsigned mask = __ballot_sync(kFull, ok);
+      if (ok) I[ni + __popc(mask & ((1u << lane) - 1))] = c;
+      ni += __popc(mask);
+    });
+    __syncwarp();
+  }
+  if (ni == 0) return 0;
+  FusedDesc fd;
+  fd.has_cond_u = fz.has_cond_u;
+  fd.cond_u_op = fz.cond_u_op;
+  const bool excl_child = fz.has_cond_u && fz.cond_u_op == VSGM_NON_EQUAL;
+  const bool other = fz.other >= 0;
+  for (uint32_t b0 = k0; b0 < n; b0 += kWarp) {
+    // pass 1, one child per lane; long slices are left for pass 2
+    const uint32_t k = b0 + lane;
+    bool heavy = false;
+    uint32_t c = 0;
+    if (k < n) {
+      c = cs[k];
+      bool sk = false;
+#pragma unroll
+      for (int i = 0; i < VSGM_MAX_QV; i++) sk |= (c == skip[i]);
+      if (!sk) {
+        uint32_t ia, ib;
+        child_slice(fd, w, I, ni, c, &ia, &ib);
+        if (ib - ia > kLaneSlice) {
+          heavy = true;
+        } else if (ia < ib) {
+          const uint64_t z0 = __ldg(rp + c + 1);
+          uint64_t cur = __ldg(rp + c), ocur = 0;
+          const uint32_t excl = excl_child ? c : 0xffffffffu;
+          for (uint32_t j = ia; j < ib; j++) {
+            const uint32_t x = I[j];
+            const uint64_t r = gallop(ci, cur, z0, x);
+            cur = r;
+            if (r < z0 && __ldg(ci + r) == x && x != excl) acc += other ? count_vs(oset, on, &ocur, x, fz.other_op) : 1ull;
+          }
+        }
+      }
+    }
+    // pass 2: the long slices of this group, one child at a time, by the whole warp
+    unsigned todo = __ballot_sync(kFull, heavy);
+    while (todo) {
+      const int src = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint32_t hc = __shfl_sync(kFull, c, src);
+      uint32_t ia, ib;
+      child_slice(fd, w, I, ni, hc, &ia, &ib);
+      const uint64_t a0 = __ldg(rp + hc), z0 = __ldg(rp + hc + 1);
+      const uint64_t s2 = lower_bound(ci, a0, z0, I[ia]);
+      const uint64_t e2 = lower_bound(ci, s2, z0, (uint64_t)I[ib - 1] + 1);
+      if (s2 >= e2) continue;
+      const uint32_t excl = excl_child ? hc : 0xffffffffu;
+      uint64_t ocur = 0;
+      if ((uint64_t)(ib - ia) <= (e2 - s2)) {
+        uint64_t cur = s2;
+        for (uint32_t j = ia + lane; j < ib; j += kWarp) {
+          const uint32_t x = I[j];
+          const uint64_t r = gallop(ci, cur, e2, x);
+          cur = r;
+          if (r < e2 && __ldg(ci + r) == x && x != excl) acc += other ? count_vs(oset, on, &ocur, x, fz.other_op) : 1ull;
+        }
+      } else {
+        uint32_t cur = ia;
+        for (uint64_t j = s2 + lane; j < e2; j += kWarp) {
+          const uint32_t x = __ldg(ci + j);
+          const uint32_t r = smem_lower_bound(I, cur, ib, x);
+          cur = r;
+          if (r < ib && I[r] == x && x != excl) acc += other ? count_vs(oset, on, &ocur, x, fz.other_op) : 1ull;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  return acc;
+}
+
 // The interpreter.  scratch: per warp, `levels` buffers of `cap` u32 (levels =
 // the longest execution sequence, cap = the largest degree of any view).
 // counts[task.plan * n_views + task.view] += matches.  *status != 0 on return
@@ -215,6 +341,9 @@ __global__ void __launch_bounds__(kDfsWarps * kWarp) k_dfs(const DfsPlan* __rest
     const DfsPlan& P = plans[task.plan];
     const DfsView V = views[task.view];
     const uint32_t n_ops = P.n_ops;
+    // a share of a split root counts the levels up to the split once (share 0 only)
+    const uint32_t split_lvl = task.c1 ? P.split_lvl : n_ops;
+    const bool first_share = task.c0 == 0;
     // stage the plan's ops in shared memory
     for (uint32_t i = lane; i < n_ops * (uint32_t)sizeof(DfsOp); i += kWarp) ((uint8_t*)O)[i] = ((const uint8_t*)P.op)[i];
     if (lane < VSGM_MAX_OPS) svisit[wib][lane] = 0;
@@ -226,14 +355,14 @@ __global__ void __launch_bounds__(kDfsWarps * kWarp) k_dfs(const DfsPlan* __rest
     for (uint64_t r = task.r0; r < task.r1 && !stopped; r++) {
       if (lane == 0) {
         S.M[P.root] = __ldg(V.sources + r);
-        svisit[wib][0]++;
+        if (first_share) svisit[wib][0]++;
       }
       __syncwarp();
       int lvl = 1;
       bool forward = true;
       while (lvl >= 1) {
         if (forward) {
-          if (lane == 0) svisit[wib][lvl]++;
+          if (lane == 0 && (first_share || (uint32_t)lvl > split_lvl)) svisit[wib][lvl]++;
           if (step_budget && ++steps > step_budget) {
             stopped = true;
             break;
@@ -265,12 +394,29 @@ __global__ void __launch_bounds__(kDfsWarps * kWarp) k_dfs(const DfsPlan* __rest
               const uint32_t* a;
               uint32_t n;
               dfs_narrow(S.set[o.u], S.len[o.u], w, &a, &n);
+              uint32_t k0 = 0;
+              if ((uint32_t)lvl == split_lvl) {  // this task's share of the root's candidates
+                n = n < task.c1 ? n : task.c1;
+                k0 = task.c0 < n ? task.c0 : n;
+              }
               S.iset[lvl] = a;
               S.ilen[lvl] = n;
-              S.inext[lvl] = 0;
+              S.inext[lvl] = k0;
               for (int i = 0; i < VSGM_MAX_QV; i++) S.ne[lvl][i] = w.ne[i];
             }
             __syncwarp();
+            if (P.fz.on && (uint32_t)lvl == P.fz.lvl) {
+              // fused tail: all children of this parent at once, then backtrack
+              const int8_t ot = P.fz.other;
+              uint64_t kids = 0;
+              acc += dfs_fused(P.fz, S.M, S.iset[lvl], S.inext[lvl], S.ilen[lvl], S.ne[lvl], ot >= 0 ? S.set[ot] : nullptr,
+                               ot >= 0 ? S.len[ot] : 0u, V.rp, V.ci, my + (uint64_t)(lvl + 1) * cap, &kids);
+              if (lane == 0 && (first_share || (uint32_t)(lvl + 1) > split_lvl)) svisit[wib][lvl + 1] += kids;
+              steps += kids;
+              forward = false;
+              lvl--;
+              continue;
+            }
           }
           // next candidate not equal to a NON_EQUAL value
           if (lane == 0) {

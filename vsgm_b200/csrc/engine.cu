@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -682,10 +683,56 @@ struct vsgm_engine {
     st->op_paths[last] += n;
   }
 
-  static DfsPlan to_dfs(const vsgm_plan& p) {
+  // the DFS fused tail (DfsFused): the level-wise engine's fusable() rule
+  static void dfs_fuse(const vsgm_plan& p, DfsPlan* d) {
+    if (p.n_ops < 3) return;
+    const int i = (int)p.n_ops - 2;
+    if (p.op_type[i] != VSGM_MATERIALIZE || p.op_type[i + 1] != VSGM_COMPUTE_COUNT) return;
+    const int u = p.op_vertex[i], w = p.op_vertex[i + 1];
+    const vsgm_vgroup& B = p.backward[w];
+    bool has_u = false;
+    for (int k = 0; k < B.count; k++) has_u |= (B.v[k] == u);
+    if (!has_u || B.count < 2 || B.count > 6) return;
+    if (p.computed_unmat[i + 1].count > 1) return;
+    const vsgm_conds& cc = p.compute_cond[w];
+    int on_u = 0;
+    for (int k = 0; k < cc.count; k++) on_u += (cc.v[k] == u);
+    if (on_u > 1) return;
+    DfsFused& f = d->fz;
+    f.on = 1;
+    f.lvl = (uint8_t)i;
+    f.other = -1;
+    f.known.type = VSGM_COMPUTE_COUNT;
+    f.known.u = (uint8_t)w;
+    for (int k = 0; k < B.count; k++)
+      if (B.v[k] != u) f.known.b[f.known.nb++] = B.v[k];
+    for (int k = 0; k < cc.count; k++) {
+      if (cc.v[k] == u) {
+        f.has_cond_u = 1;
+        f.cond_u_op = cc.op[k];
+      } else {
+        f.known.cop[f.known.nc] = cc.op[k];
+        f.known.cv[f.known.nc++] = cc.v[k];
+      }
+    }
+    const vsgm_vgroup& cu = p.computed_unmat[i + 1];
+    if (cu.count == 1) {
+      f.other = (int8_t)cu.v[0];
+      f.other_op = p.order[w][cu.v[0]];
+    }
+  }
+
+  static DfsPlan to_dfs(const vsgm_plan& p, bool fuse = true) {
     DfsPlan d;
     std::memset(&d, 0, sizeof(d));
+    if (fuse) dfs_fuse(p, &d);
     d.n_ops = p.n_ops;
+    d.split_lvl = p.n_ops;
+    for (uint32_t i = 1; i < p.n_ops; i++)
+      if (p.op_type[i] == VSGM_MATERIALIZE) {
+        d.split_lvl = i;
+        break;
+      }
     d.root = p.op_vertex[0];
     for (uint32_t i = 0; i < p.n_ops; i++) {
       DfsOp& o = d.op[i];
@@ -729,7 +776,7 @@ struct vsgm_engine {
     std::vector<DfsPlan> hp(n_plans);
     uint32_t levels = 1;
     for (int k = 0; k < n_plans; k++) {
-      hp[k] = to_dfs(plans[plan_ids[k]]);
+      hp[k] = to_dfs(plans[plan_ids[k]], knobs[plan_ids[k]].fuse_tail);
       levels = std::max(levels, hp[k].n_ops);
     }
     std::vector<DfsView> hv(n_views);
@@ -752,12 +799,26 @@ struct vsgm_engine {
     for (int pk = 0; pk < n_plans; pk++)
       for (int k = 0; k < n_views; k++) {
         const auto& deg = rviews[view_ids[k]].h_deg_src;
+        const bool splittable = hp[pk].split_lvl < hp[pk].n_ops;
         uint64_t r0 = 0;
         double acc = 0;
         for (uint64_t r = 0; r < deg.size(); r++) {
-          acc += (double)deg[r] * (double)deg[r] + 1.0;
+          const double w = (double)deg[r] * (double)deg[r] + 1.0;
+          if (splittable && w > 2.0 * target && deg[r] > 1) {
+            // a heavy root: close the open range, then split the root's candidates at
+            // the split level (a subset of its neighbours) into shares of ~target work
+            if (r > r0) tasks.push_back({acc, DfsTask{(uint32_t)pk, (uint32_t)k, r0, r, 0u, 0u}});
+            const uint64_t shares = std::min<uint64_t>(deg[r], (uint64_t)std::ceil(w / target));
+            const uint64_t per = (deg[r] + shares - 1) / shares;
+            for (uint64_t c0 = 0; c0 < deg[r]; c0 += per)
+              tasks.push_back({w / (double)shares, DfsTask{(uint32_t)pk, (uint32_t)k, r, r + 1, (uint32_t)c0, (uint32_t)std::min<uint64_t>(c0 + per, deg[r])}});
+            r0 = r + 1;
+            acc = 0;
+            continue;
+          }
+          acc += w;
           if (acc >= target || r + 1 == deg.size()) {
-            tasks.push_back({acc, DfsTask{(uint32_t)pk, (uint32_t)k, r0, r + 1}});
+            tasks.push_back({acc, DfsTask{(uint32_t)pk, (uint32_t)k, r0, r + 1, 0u, 0u}});
             r0 = r + 1;
             acc = 0;
           }
@@ -1286,6 +1347,8 @@ constexpr size_t kNoAllocDescOff = 256;
 constexpr size_t kNoAllocTaskOff = 1280;
 constexpr size_t kNoAllocScratchOff = (kNoAllocTaskOff + kNoAllocMaxTasks * sizeof(DfsTask) + 255) & ~(size_t)255;
 constexpr uint64_t kNoAllocWarpU32 = (kNoAllocBytes - kNoAllocScratchOff) / (kNoAllocWarps * sizeof(uint32_t));
+static_assert(sizeof(DfsPlan) + sizeof(DfsView) <= kNoAllocTaskOff - kNoAllocDescOff, "plan + view must fit their slot");
+static_assert(kNoAllocWarpU32 == 24319, "the documented limit (plan ops x max degree) follows the layout");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -1317,7 +1380,7 @@ __global__ void k_noalloc_max_degree(const uint64_t* __restrict__ rp, uint64_t V
 __global__ void k_noalloc_tasks(DfsTask* tasks, uint64_t n_tasks, uint64_t n_sources, uint64_t chunk) {
   for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_tasks; t += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t r0 = t * chunk;
-    tasks[t] = DfsTask{0u, 0u, r0, r0 + chunk < n_sources ? r0 + chunk : n_sources};
+    tasks[t] = DfsTask{0u, 0u, r0, r0 + chunk < n_sources ? r0 + chunk : n_sources, 0u, 0u};
   }
 }
 

@@ -5,8 +5,9 @@ The reference picks one search sequence per pattern with a fixed heuristic
 predicts, for a (pattern, view) pair, the log intermediate-result size of every
 candidate search sequence, and the planner runs the predicted cheapest one.  The
 network only chooses the plan: every order of a pattern yields the same exact
-count, and the heuristic order is kept whenever the predicted gain is below a
-confidence margin.
+count.  choose() trusts the prediction beyond a confidence margin;
+choose_verified() (the planner's default) lets the network propose a few orders
+and keeps the heuristic one unless a sampled run of the proposals beats it.
 
 Features (76 values):
   36  pattern adjacency bits (6 x 6, after the query's vertex re-mapping)
@@ -197,6 +198,33 @@ class LearnedPlanner:
         y = np.zeros((len(X), N_OUT), np.float32)
         capi.check(self.L.vsgm_mlp_forward(self.h, self._p(X), len(X), y.ctypes.data_as(C.POINTER(C.c_float))))
         return y
+
+    def propose(self, plan, x, k=4):
+        """The k valid orders with the lowest predicted cost (heuristic order excluded)."""
+        pred = self.predict(x[None, :])[0]
+        h = heuristic_order(plan)
+        ranked = sorted((o for o in valid_orders(plan) if o != h), key=lambda o: pred[order_index(o)])
+        return ranked[:k]
+
+    def choose_verified(self, plan, sampler, view_index, k=4, margin=0.05):
+        """(order, used_model): the network proposes its k cheapest-looking orders, one
+        batched run over the view's root sample measures them beside the heuristic
+        order, and the measured cheapest wins if it does at least `margin` (relative)
+        less work than the heuristic; otherwise the heuristic order is kept.  A wrong
+        prediction therefore costs one sampled run, never a slow full run."""
+        h = heuristic_order(plan)
+        _, lvl0, _ = sampler.evaluate([plan], view_index)
+        x = features(plan, sampler.hist[view_index], lvl0[0][0])
+        cands = [h] + self.propose(plan, x, k)
+        plans = [plan_reorder(plan, o) for o in cands]
+        _, lvl, ovf = sampler.evaluate(plans, view_index)
+        work = [sum(int(lvl[i][0][j]) for j in range(plans[i].n_ops)) for i in range(len(plans))]
+        # an order stopped by the step budget did at least that much work: never prefer it
+        work = [w if not ovf[i][0] else float("inf") for i, w in enumerate(work)]
+        best = min(range(len(cands)), key=lambda i: work[i])
+        if best != 0 and work[best] < (1.0 - margin) * work[0]:
+            return cands[best], True
+        return h, False
 
     def choose(self, plan, x, margin=0.25):
         """(order, used_model): the predicted cheapest valid order, or the heuristic
