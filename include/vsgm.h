@@ -224,6 +224,8 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   rooted at each cycle's largest vertex (sum over opposite vertices of
  *   C(wedges, 2)) instead of the plan's op sequence; totals are identical, per-view
  *   counts are attributed to the largest instead of the smallest vertex;
+ *   "c4_heavy" (default 2^20): roots with at least this many wedges are counted by
+ *   groups sharing the whole GPU with L2-resident counters (0: every root);
  *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT
  *   of a vertex with the same backward lists and conditions (the diamond's tail)
  *   counts the pairs of one intersection instead of intersecting twice;

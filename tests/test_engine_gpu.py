@@ -284,6 +284,7 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
         assert e.counts() == want
         e.set_option("root_stride", 3)
         e.set_option("only_plan", 1)
+        e.set_option("c4_aggregate", 0)  # a root sample counts like the plan only without aggregation
         e.reset_counts()
         e.match()
         assert e.counts()[1] == orc.count(plans[1], g, np.arange(0, g.V, 3, dtype=np.uint32))
@@ -296,12 +297,13 @@ def test_four_cycle_aggregation_equals_plan(vs, orc, graphs):
     for g in (graphs["rmat7"], graphs["rmat8"], graphs["chunglu"], vs.degree_relabel(graphs["rmat8"])[0],
               vs.degree_relabel(graphs["rmat8"], ascending=False)[0], hub, cycle_graph(vs, 4), complete_graph(vs, 6)):
         want = orc.count(p, g)
-        for agg in (1, 0):
+        for agg, heavy in ((1, 1 << 20), (1, 0), (1, 64), (0, 0)):
             with vs.Engine(g.V, [p]) as e:
                 e.set_option("c4_aggregate", agg)
+                e.set_option("c4_heavy", heavy)  # 0: every root through the group kernels
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
                 e.match()
-                assert e.counts() == [want], agg
+                assert e.counts() == [want], (agg, heavy)
     # views: per-view attribution differs, totals do not
     g = graphs["rmat8"]
     bins = (np.arange(g.V) % 3).astype(np.int32)

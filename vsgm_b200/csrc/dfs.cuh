@@ -279,8 +279,8 @@ __device__ __forceinline__ unsigned long long dfs_fused(const DfsFused& fz, cons
       uint32_t ia, ib;
       child_slice(fd, w, I, ni, hc, &ia, &ib);
       const uint64_t a0 = __ldg(rp + hc), z0 = __ldg(rp + hc + 1);
-      const uint64_t s2 = lower_bound(ci, a0, z0, I[ia]);
-      const uint64_t e2 = lower_bound(ci, s2, z0, (uint64_t)I[ib - 1] + 1);
+      const uint64_t s2 = warp_lower_bound(ci, a0, z0, I[ia]);
+      const uint64_t e2 = warp_lower_bound(ci, s2, z0, (uint64_t)I[ib - 1] + 1);
       if (s2 >= e2) continue;
       const uint32_t excl = excl_child ? hc : 0xffffffffu;
       uint64_t ocur = 0;

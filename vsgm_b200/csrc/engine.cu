@@ -116,6 +116,7 @@ struct vsgm_engine {
     bool lane_merge = false;         // counting kernels: lane-partitioned merge
     bool c4_aggregate = true;        // 4-cycle plans: wedge aggregation instead of the op sequence
     bool set_reuse = true;           // COMPUTE o + COMPUTE_COUNT w over the same set: count pairs of one intersection
+    uint64_t c4_heavy = 1ull << 20;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -661,25 +662,80 @@ struct vsgm_engine {
     return true;
   }
 
-  // 4-cycles rooted at the given sources, by wedge aggregation (k_c4_aggregate);
-  // each cycle is attributed to its largest vertex, the plan attributes it to its
-  // smallest: totals over all sources are the same
+  // 4-cycles rooted at the given sources, by wedge aggregation; each cycle is
+  // attributed to its largest vertex, the plan attributes it to its smallest:
+  // totals over all sources are the same.  Roots with at least kC4Heavy wedges
+  // (most of the work on skewed graphs) go through the L2-resident group kernels,
+  // the rest through k_c4_aggregate (one root per block).  Threshold: the
+  // per-plan knob c4_heavy (default 2^20 wedges).
   void c4_aggregate(const uint32_t* roots, uint64_t n) {
     const int last = (int)plan->n_ops - 1;
     Mark m(arena);
-    const uint64_t per_block = 2ull * V * sizeof(uint32_t);
-    uint64_t blocks = std::min<uint64_t>((uint64_t)sms * 4, (arena.avail() > (1u << 20) ? arena.avail() - (1u << 20) : 0) / per_block);
-    if (blocks == 0) throw OutOfMemory{"HBM budget exhausted (4-cycle counters)"};
-    blocks = std::min<uint64_t>(blocks, std::max<uint64_t>(1, n));
-    uint32_t* L = arena.take_n<uint32_t>(blocks * V, "4-cycle counters");
-    uint32_t* touched = arena.take_n<uint32_t>(blocks * V, "4-cycle touched ids");
-    unsigned long long* head = arena.take_n<unsigned long long>(1, "4-cycle queue head");
     begin_op();
-    CK(cudaMemsetAsync(L, 0, blocks * V * sizeof(uint32_t), stream));
-    CK(cudaMemsetAsync(head, 0, sizeof(unsigned long long), stream));
-    k_c4_aggregate<<<(unsigned)blocks, 256, 0, stream>>>(d_rp, d_ci, roots, n, V, L, touched, head, d_total);
+    // split the roots by wedge count
+    unsigned long long* W = arena.take_n<unsigned long long>(V, "4-cycle wedge counts");
+    uint32_t* heavy = arena.take_n<uint32_t>(std::max<uint64_t>(n, 1), "4-cycle heavy roots");
+    uint64_t* centres = arena.take_n<uint64_t>(std::max<uint64_t>(n, 1), "4-cycle wedge centres");
+    uint32_t* light = arena.take_n<uint32_t>(std::max<uint64_t>(n, 1), "4-cycle light roots");
+    unsigned long long* ctr = arena.take_n<unsigned long long>(2, "4-cycle split counters");
+    CK(cudaMemsetAsync(W, 0, V * sizeof(unsigned long long), stream));
+    CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), stream));
+    k_c4_wedge_counts<<<grid_warps(V), 256, 0, stream>>>(d_rp, d_ci, V, W);
+    k_c4_split<<<grid_threads(n), 256, 0, stream>>>(d_rp, d_ci, roots, n, W, cur.c4_heavy, heavy, centres, light, ctr);
     CK(cudaGetLastError());
-    end_op(last, 1);
+    CK(cudaMemcpyAsync(h_pinned, ctr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    const uint64_t n_heavy = h_pinned[0], n_light = h_pinned[1];
+    uint64_t launches = 2;
+    if (n_light) {
+      launches++;
+      const uint64_t per_block = 2ull * V * sizeof(uint32_t);
+      uint64_t blocks = std::min<uint64_t>((uint64_t)sms * 4, (arena.avail() > (1u << 20) ? arena.avail() - (1u << 20) : 0) / per_block);
+      if (blocks == 0) throw OutOfMemory{"HBM budget exhausted (4-cycle counters)"};
+      blocks = std::min<uint64_t>(blocks, n_light);
+      Mark ml(arena);
+      uint32_t* L = arena.take_n<uint32_t>(blocks * V, "4-cycle counters");
+      uint32_t* touched = arena.take_n<uint32_t>(blocks * V, "4-cycle touched ids");
+      unsigned long long* head = arena.take_n<unsigned long long>(1, "4-cycle queue head");
+      CK(cudaMemsetAsync(L, 0, blocks * V * sizeof(uint32_t), stream));
+      CK(cudaMemsetAsync(head, 0, sizeof(unsigned long long), stream));
+      k_c4_aggregate<<<(unsigned)blocks, 256, 0, stream>>>(d_rp, d_ci, light, n_light, V, L, touched, head, d_total);
+      CK(cudaGetLastError());
+    }
+    if (n_heavy) {
+      std::vector<uint32_t> hr(n_heavy);
+      std::vector<uint64_t> hc(n_heavy);
+      CK(cudaMemcpyAsync(hr.data(), heavy, n_heavy * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+      CK(cudaMemcpyAsync(hc.data(), centres, n_heavy * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      // groups of up to kC4Group roots whose counter arrays fit in about 96 MB (L2)
+      const uint64_t stride = (V + 3) & ~3ull;
+      const uint64_t per_root = stride * sizeof(uint32_t);
+      const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>(kC4Group, (96ull << 20) / per_root));
+      std::vector<C4Group> groups;
+      for (uint64_t k = 0; k < n_heavy; k += G) {
+        C4Group g;
+        std::memset(&g, 0, sizeof(g));
+        g.n = (uint32_t)std::min<uint64_t>(G, n_heavy - k);
+        for (uint32_t i = 0; i < g.n; i++) {
+          g.root[i] = hr[k + i];
+          g.vbeg[i + 1] = g.vbeg[i] + hc[k + i];
+        }
+        groups.push_back(g);
+      }
+      C4Group* d_groups = arena.take_n<C4Group>(groups.size(), "4-cycle groups");
+      uint32_t* L = arena.take_n<uint32_t>((uint64_t)G * stride, "4-cycle group counters");
+      CK(cudaMemcpyAsync(d_groups, groups.data(), groups.size() * sizeof(C4Group), cudaMemcpyHostToDevice, stream));
+      CK(cudaMemsetAsync(L, 0, (uint64_t)G * per_root, stream));
+      const unsigned gw = (unsigned)sms * 8, gs = (unsigned)sms * 4;
+      for (size_t i = 0; i < groups.size(); i++) {
+        k_c4_group_wedges<<<gw, 256, 0, stream>>>(d_rp, d_ci, d_groups + i, L, stride);
+        k_c4_group_sum<<<gs, 256, 0, stream>>>(d_groups + i, L, stride, d_total);
+      }
+      CK(cudaGetLastError());
+      launches += 2 * groups.size();
+    }
+    end_op(last, launches);
     st->op_paths[last] += n;
   }
 
@@ -1201,6 +1257,11 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   }
   if (n == "c4_aggregate") {
     for (int k = lo; k < hi; k++) e->knobs[k].c4_aggregate = value != 0;
+    return VSGM_OK;
+  }
+  if (n == "c4_heavy") {
+    if (value < 0) return engine_fail(e, VSGM_EINVAL, "c4_heavy must be >= 0");
+    for (int k = lo; k < hi; k++) e->knobs[k].c4_heavy = (uint64_t)value;
     return VSGM_OK;
   }
   if (n == "lane_merge") {

@@ -92,6 +92,26 @@ __device__ __forceinline__ uint64_t lower_bound(const uint32_t* __restrict__ a, 
 }
 
 // Per-path condition state: candidates must lie in [lo, hi) and differ from ne[].
+// Lower bound by the whole warp: every round the 32 lanes probe 32 evenly spaced
+// positions of [lo, hi), so a range of n shrinks to n/32 per round (4 rounds of
+// independent loads for 10^6 elements instead of 20 dependent ones).  All lanes
+// must call it with the same arguments; all get the same result.
+__device__ __forceinline__ uint64_t warp_lower_bound(const uint32_t* __restrict__ a, uint64_t lo, uint64_t hi, uint64_t x) {
+  const unsigned lane = lane_id();
+  while (hi - lo > kWarp) {
+    const uint64_t step = (hi - lo + kWarp - 1) / kWarp;
+    const uint64_t p = lo + lane * step;
+    const unsigned below = __ballot_sync(kFull, p < hi && (uint64_t)__ldg(a + p) < x);
+    const unsigned cnt = __popc(below);  // a prefix of the lanes: the array is sorted
+    if (cnt == 0) return lo;
+    const uint64_t nhi = lo + cnt * step;
+    lo = lo + (cnt - 1) * step + 1;
+    if (nhi < hi) hi = nhi;
+  }
+  const uint64_t p = lo + lane;
+  return lo + __popc(__ballot_sync(kFull, p < hi && (uint64_t)__ldg(a + p) < x));
+}
+
 struct Window {
   uint64_t lo, hi;
   uint32_t ne[VSGM_MAX_QV];
@@ -632,8 +652,8 @@ __global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const 
           uint32_t ia, ib;
           child_slice(fd, w, I, ni, c, &ia, &ib);
           const uint64_t a0 = __ldg(rp + c), z0 = __ldg(rp + c + 1);
-          const uint64_t s2 = lower_bound(ci, a0, z0, I[ia]);
-          const uint64_t e2 = lower_bound(ci, s2, z0, (uint64_t)I[ib - 1] + 1);
+          const uint64_t s2 = warp_lower_bound(ci, a0, z0, I[ia]);
+          const uint64_t e2 = warp_lower_bound(ci, s2, z0, (uint64_t)I[ib - 1] + 1);
           if (lane == 0) acc_bytes += 4ull * ((uint64_t)(ib - ia) < e2 - s2 ? (uint64_t)(ib - ia) : e2 - s2) + 16ull;
           if (s2 >= e2) continue;
           const uint32_t excl = excl_child ? c : 0xffffffffu;
@@ -832,6 +852,92 @@ __global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict
     for (unsigned i = 0; i < nwarps; i++) t += s_sum[i];
     if (t) atomicAdd(total, t);
   }
+}
+
+// Heavy roots of the same count.  A root u with many wedges is shared by the whole
+// GPU: a group of G such roots keeps G dense counter arrays (one per root, over the
+// ids below u) small enough to stay in L2, every warp takes one wedge centre v of
+// one root and adds its wedges with fire-and-forget atomics (no return value, so no
+// touched list), and a second pass sums C(L[w], 2) over [0, u) and clears the
+// counters for the next group.
+struct C4Group {
+  uint32_t n;                  // roots in the group (<= kC4Group)
+  uint32_t root[8];
+  uint64_t vbeg[9];            // prefix of the wedge centres (neighbours below the root) per root
+};
+constexpr int kC4Group = 8;
+
+__device__ __forceinline__ unsigned long long pairs_of(uint32_t c) { return (unsigned long long)c * (c ? c - 1u : 0u) / 2; }
+
+// W[u] += wedges that end at u's lower neighbours: for every edge v-u with v < u,
+// the number of neighbours of v below u (u's position in v's sorted row)
+__global__ void k_c4_wedge_counts(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t V, unsigned long long* __restrict__ W) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; v < V; v += warps) {
+    const uint64_t a = __ldg(rp + v), z = __ldg(rp + v + 1);
+    for (uint64_t j = a + lane; j < z; j += kWarp) {
+      const uint32_t u = __ldg(ci + j);
+      if (u > v && j > a) atomicAdd(W + u, (unsigned long long)(j - a));
+    }
+  }
+}
+
+// split roots by wedge count; centres[k] = neighbours of heavy root k below it
+__global__ void k_c4_split(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ roots, uint64_t n,
+                           const unsigned long long* __restrict__ W, unsigned long long threshold, uint32_t* __restrict__ heavy,
+                           uint64_t* __restrict__ centres, uint32_t* __restrict__ light, unsigned long long* __restrict__ counters) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = roots[i];
+    if (W[u] >= threshold) {
+      const unsigned long long k = atomicAdd(counters, 1ull);
+      heavy[k] = u;
+      centres[k] = lower_bound(ci, __ldg(rp + u), __ldg(rp + u + 1), u) - __ldg(rp + u);
+    } else {
+      light[atomicAdd(counters + 1, 1ull)] = u;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_c4_group_wedges(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const C4Group* __restrict__ grp,
+                                                         uint32_t* __restrict__ L, uint64_t stride) {
+  const C4Group& G = *grp;
+  const uint64_t total = G.vbeg[G.n];
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < total; i += warps) {
+    uint32_t g = 0;
+    while (g + 1 < G.n && i >= G.vbeg[g + 1]) g++;
+    const uint32_t u = G.root[g];
+    const uint32_t v = __ldg(ci + __ldg(rp + u) + (i - G.vbeg[g]));  // v < u: the row is sorted
+    uint32_t* Lg = L + (uint64_t)g * stride;
+    const uint64_t z = __ldg(rp + v + 1);
+    for (uint64_t base = __ldg(rp + v); base < z; base += kWarp) {
+      const uint64_t j = base + lane;
+      const uint32_t w = j < z ? __ldg(ci + j) : u;
+      if (w < u) atomicAdd(Lg + w, 1u);
+      if (__any_sync(kFull, w >= u)) break;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_c4_group_sum(const C4Group* __restrict__ grp, uint32_t* __restrict__ L, uint64_t stride,
+                                                      unsigned long long* __restrict__ total) {
+  const C4Group& G = *grp;
+  unsigned long long acc = 0;
+  for (uint32_t g = 0; g < G.n; g++) {
+    uint4* Lg = (uint4*)(L + (uint64_t)g * stride);
+    const uint64_t n4 = ((uint64_t)G.root[g] + 3) / 4;  // counters below the root, rounded up (the rest are zero)
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += (uint64_t)gridDim.x * blockDim.x) {
+      const uint4 c = Lg[k];
+      if (c.x | c.y | c.z | c.w) {
+        acc += pairs_of(c.x) + pairs_of(c.y) + pairs_of(c.z) + pairs_of(c.w);
+        Lg[k] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if ((threadIdx.x & (kWarp - 1)) == 0 && acc) atomicAdd(total, acc);
 }
 
 // ---------------------------------------------------------------------------
