@@ -1,0 +1,78 @@
+"""The workload configurations at their full sizes (c1, c2) and the large one when
+asked for (c5, VSGM_LARGE=1): exact counts against the oracle where it finishes
+in seconds (c1 whole graph, c2 on a random root sample), and size-independent
+checks at full size (interleaved source bins sum to the whole-graph total; the
+totals do not depend on the vertex labelling).
+"""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# whole-graph totals of the R-MAT scale-22 workload (-kc 4, -p 1, -p 2); the same
+# under native, degree-ascending and degree-descending ids
+C2_COUNTS = [124_023_930_675, 3_848_799_057_616, 3_080_671_377_357]
+
+
+def test_c1_triangles_rmat16(vs, orc):
+    from vsgm_b200 import workloads as wl
+    g, plans = wl.triangle_rmat16()
+    want = orc.count(plans[0], g)
+    for asc in (True, False):
+        h, _ = vs.degree_relabel(g, ascending=asc)
+        assert vs.count_graph(h, plans) == [want]
+    assert vs.count_graph(g, plans) == [want]
+
+
+@pytest.fixture(scope="module")
+def rmat22(vs):
+    from vsgm_b200 import workloads as wl
+    g, plans = wl.patterns_rmat22()
+    h, _ = vs.degree_relabel(g, ascending=True)
+    return h, plans
+
+
+def test_c2_whole_graph_and_bins(vs, rmat22):
+    g, plans = rmat22
+    assert vs.count_graph(g, plans) == C2_COUNTS
+    with vs.Engine(g.V, plans) as e:
+        e.upload_graph(g)
+        for b in range(4):
+            e.graph_view(np.arange(b, g.V, 4, dtype=np.uint32))
+            e.match()
+        assert e.counts() == C2_COUNTS
+
+
+def test_c2_root_sample_against_oracle(vs, orc, rmat22):
+    g, plans = rmat22
+    rng = np.random.default_rng(21)
+    src = np.sort(rng.choice(g.V, size=3000, replace=False)).astype(np.uint32)
+    with vs.Engine(g.V, plans) as e:
+        e.set_option("c4_aggregate", 0)  # per-root attribution of the plan
+        e.transfer_view(g, src)
+        e.match()
+        got = e.counts()
+    assert got == [orc.count(p, g, src) for p in plans]
+
+
+@pytest.mark.skipif(os.environ.get("VSGM_LARGE") != "1", reason="65M-vertex graph: set VSGM_LARGE=1")
+def test_c5_large_chung_lu(vs, orc):
+    from vsgm_b200 import workloads as wl
+    g = wl.social_chung_lu()
+    g, _ = vs.degree_relabel(g, ascending=True)
+    plans = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(4)]
+    whole = vs.count_graph(g, plans)
+    with vs.Engine(g.V, plans) as e:
+        e.upload_graph(g)
+        rng = np.random.default_rng(5)
+        src = np.sort(rng.choice(g.V, size=2000, replace=False)).astype(np.uint32)
+        e.graph_view(src)
+        e.match()
+        assert e.counts() == [orc.count(p, g, src) for p in plans]
+        e.reset_counts()
+        for b in range(4):
+            e.graph_view(np.arange(b, g.V, 4, dtype=np.uint32))
+            e.match()
+        assert e.counts() == whole

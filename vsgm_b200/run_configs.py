@@ -1,0 +1,188 @@
+"""Run one of the five workload configurations on one GPU; print one JSON line.
+
+    python -m vsgm_b200.run_configs c1 | c3 | c4 | c5 [options]
+
+c1  -kc 3 on R-MAT scale 16, edge factor 16, seed 1, ids ascending with degree
+    (the degree-ordered orientation), one view holding every source.
+c3  64 random connected patterns (3-6 vertices, p = 0.5, seed 3) x 16 Chung-Lu
+    views (exponent U[2.1, 2.8], edges log-uniform in [1e5, e_max], max degree
+    1e4, seed 3): the persistent batched launch against the plain level-wise
+    engine view after view, at identical counts.  Patterns whose sampled work
+    exceeds --max-work on some view are left out and listed.
+c4  the learned planner on c3-distributed (pattern, view) pairs (seed 4): the
+    network is trained by the library's MLP kernels on measured per-op work of
+    candidate orders; held-out pairs report the work of the heuristic order and
+    of the verified learned choice on an independent root sample.
+c5  Chung-Lu, 65M vertices, ~1.8B edges, exponent 2.2, max degree 5000, seed 5
+    (use --scale-down k for a 1/k-size graph of the same shape): -kc 3, -kc 4,
+    -p 4 (house), whole graph as one view, plus the same totals over 4
+    interleaved source bins as a size-independent consistency check.
+
+Counts are exact u64; times are device times from the engine's CUDA events
+(value) and wall time around the C ABI calls (wall).  No oracle is used here:
+parity is the test suite's job.
+"""
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+from . import Engine, Graph, degree_relabel, gen_rmat, plan_clique, plan_pattern
+from . import planner as lp
+from . import workloads as wl
+
+
+def _match_all(g, plans, device=0, sources=None, options=()):
+    src = np.arange(g.V, dtype=np.uint32) if sources is None else sources
+    with Engine(g.V, plans, device=device) as e:
+        for k, v in options:
+            e.set_option(k, v)
+        e.transfer_view(g, src)
+        e.set_profiling(True)
+        e.match()  # warm-up (first-touch of the arena, module load)
+        e.reset_counts()
+        t = time.perf_counter()
+        e.match()
+        wall = time.perf_counter() - t
+        per = []
+        for i, p in enumerate(plans):
+            s = e.stats(i)
+            per.append(sum(s.op_ms[j] for j in range(p.n_ops)))
+        return e.counts(), per, wall
+
+
+def run_c1(args):
+    g = gen_rmat(16, 16, *wl.RMAT_ABC, seed=1)
+    g, _ = degree_relabel(g, ascending=True)
+    counts, per, wall = _match_all(g, [plan_clique(3)])
+    return {"config": "c1", "graph": f"R-MAT 16 ef16 seed 1, V={g.V}, E={g.E}", "query": "-kc 3", "count": counts[0],
+            "device_ms": per[0], "wall_ms": wall * 1e3, "matches_per_s": counts[0] / (per[0] / 1e3) if per[0] else None}
+
+
+def _screen(plans, views, stride, step_budget, device=0):
+    V = max(g.V for g in views)
+    with Engine(V, plans, device=device) as e:
+        ids = [e.add_view(g, np.arange(0, g.V, stride, dtype=np.uint32)) for g in views]
+        cnt, lvl, ovf = e.run_batched_ex(ids, step_budget=step_budget)
+    return lvl.sum(axis=2) * stride, ovf
+
+
+def run_c3(args):
+    views = [degree_relabel(g)[0] for g in wl.chung_lu_views(16, seed=3, e_max=args.e_max)]
+    pats = wl.random_patterns(64, seed=3)
+    work, ovf = _screen(pats, views, stride=97, step_budget=200_000)
+    keep = [i for i in range(len(pats)) if not ovf[i].any() and work[i].max() < args.max_work]
+    plans = [pats[i] for i in keep]
+    V = max(g.V for g in views)
+    # batched: every (pattern, view) pair in one persistent launch
+    with Engine(V, plans) as e:
+        ids = [e.add_view(g) for g in views]
+        e.set_profiling(True)
+        e.run_batched(ids)  # warm-up
+        t = time.perf_counter()
+        batched = e.run_batched(ids)
+        b_wall = time.perf_counter() - t
+        st = e.batch_stats()
+        b_ms, tasks = st.ms, st.tasks
+    # plain: the level-wise engine, one view after the other (uploads outside the timing)
+    plain = [[0] * len(views) for _ in plans]
+    p_ms = p_wall = 0.0
+    launches = 0
+    with Engine(V, plans) as e:
+        e.set_profiling(True)
+        for vi, g in enumerate(views):
+            rp = np.concatenate([g.row_ptrs, np.full(V - g.V, g.row_ptrs[-1], np.uint64)])
+            e.transfer_view(Graph(rp, g.cols), np.arange(g.V, dtype=np.uint32))
+            e.reset_counts()
+            t = time.perf_counter()
+            e.match()
+            p_wall += time.perf_counter() - t
+            c = e.counts()
+            for pi, p in enumerate(plans):
+                plain[pi][vi] = c[pi]
+                s = e.stats(pi)
+                p_ms += sum(s.op_ms[j] for j in range(p.n_ops))
+                launches += sum(s.op_launches[j] for j in range(p.n_ops))
+    total = sum(sum(r) for r in plain)
+    return {"config": "c3", "views": [(g.V, g.E) for g in views], "patterns_run": len(keep), "patterns_left_out": [i for i in range(len(pats)) if i not in keep],
+            "identical_counts": [list(map(int, r)) for r in batched] == plain, "matches": int(total),
+            "batched": {"device_ms": b_ms, "wall_ms": b_wall * 1e3, "launches": 1, "tasks": int(tasks)},
+            "plain": {"device_ms": p_ms, "wall_ms": p_wall * 1e3, "launches": int(launches)},
+            "speedup_wall": p_wall / b_wall if b_wall else None}
+
+
+def run_c4(args):
+    views = [degree_relabel(g)[0] for g in wl.chung_lu_views(args.views, seed=4, e_min=2e4, e_max=args.e_max, max_degree=2000)]
+    pats = wl.random_patterns(args.patterns, seed=4)
+    sampler = lp.Sampler(views, roots_per_view=256, seed=1, step_budget=500_000)
+    check = lp.Sampler(views, roots_per_view=256, seed=99, step_budget=4_000_000)
+    pairs = [(pi, vi) for pi in range(len(pats)) for vi in range(len(views))]
+    rng = np.random.default_rng(0)
+    rng.shuffle(pairs)
+    cut = int(0.8 * len(pairs))
+    t = time.perf_counter()
+    X, Y, M, _ = lp.make_examples(sampler, pats, pairs[:cut], orders_per_pair=8, seed=1)
+    t_logs = time.perf_counter() - t
+    model = lp.LearnedPlanner()
+    t = time.perf_counter()
+    losses = model.train(X, Y, M, epochs=150)
+    t_train = time.perf_counter() - t
+    heur = learned = 0.0
+    used = 0
+    for pi, vi in pairs[cut:]:
+        base = pats[pi]
+        order, took = model.choose_verified(base, sampler, vi, k=4)
+        used += took
+        plans = [lp.plan_reorder(base, lp.heuristic_order(base)), lp.plan_reorder(base, order)]
+        cnt, lvl, ovf = check.evaluate(plans, vi)
+        heur += sum(int(x) for x in lvl[0][0][:plans[0].n_ops])
+        learned += sum(int(x) for x in lvl[1][0][:plans[1].n_ops])
+    model.close()
+    return {"config": "c4", "train_pairs": cut, "held_out_pairs": len(pairs) - cut, "examples": int(len(X)), "log_s": t_logs, "train_s": t_train,
+            "loss_first": losses[0], "loss_last": losses[-1], "model_order_used": used,
+            "held_out_work": {"heuristic": heur, "learned": learned, "gain": heur / learned if learned else None}}
+
+
+def run_c5(args):
+    k = args.scale_down
+    t = time.perf_counter()
+    g = wl.social_chung_lu(V=65_000_000 // k, edges=1_800_000_000 // k)
+    g, _ = degree_relabel(g, ascending=True)
+    t_gen = time.perf_counter() - t
+    plans = [plan_clique(3), plan_clique(4), plan_pattern(4)]
+    counts, per, wall = _match_all(g, plans)
+    # the same totals over 4 interleaved source bins
+    bins = [np.arange(b, g.V, 4, dtype=np.uint32) for b in range(4)]
+    with Engine(g.V, plans) as e:
+        e.upload_graph(g)  # resident once; every bin is matched over it (no halo needed)
+        t = time.perf_counter()
+        for b in bins:
+            e.graph_view(b)
+            e.match()
+        bins_wall = time.perf_counter() - t
+        tot = e.counts()
+    return {"config": "c5", "graph": f"Chung-Lu V={g.V} E={g.E} (exponent 2.2, max degree 5000, seed 5)", "scale_down": k, "gen_s": t_gen,
+            "queries": ["-kc 3", "-kc 4", "-p 4"], "counts": counts, "device_ms": per, "wall_ms": wall * 1e3,
+            "bins_total_equal": tot == counts, "bins_wall_ms": bins_wall * 1e3}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("config", choices=["c1", "c3", "c4", "c5"])
+    ap.add_argument("--e-max", type=float, default=None)
+    ap.add_argument("--max-work", type=float, default=5e9)
+    ap.add_argument("--views", type=int, default=8)
+    ap.add_argument("--patterns", type=int, default=96)
+    ap.add_argument("--scale-down", type=int, default=1)
+    args = ap.parse_args(argv)
+    if args.e_max is None:
+        args.e_max = {"c3": 1e7, "c4": 2e5}.get(args.config, 1e7)
+    out = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
