@@ -103,6 +103,30 @@ def test_view_materialize_matches_halo(vs, hop, root_degree):
             assert len(row) == 0
 
 
+def _ref_views():
+    return np.load(os.path.join(ROOT, "tests", "golden", "ref_views.npz"))
+
+
+def test_view_materialize_matches_reference_golden(vs, tmp_path):
+    """Byte-identical to the reference's own ViewBin::Materialize (fixture made by
+    tests/golden/make_view_golden.py from the reference sources), and our .bin file
+    reads back in the reference reader with the same V, E and column sum."""
+    z = _ref_views()
+    g = vs.Graph(z["row_ptrs"], z["cols"])
+    V, E, colsum = (int(x) for x in z["read"])
+    assert (g.V, g.E, int(g.cols.astype(np.uint64).sum())) == (V, E, colsum)
+    path = tmp_path / "g.bin"
+    vs.write_csr_bin(path, g)
+    h = vs.read_csr_bin(path)
+    assert np.array_equal(h.row_ptrs, g.row_ptrs) and np.array_equal(h.cols, g.cols)
+    src = vs.sources_of_bins(z["bins"], 3)
+    for c, (hop, rd) in enumerate(z["cases"]):
+        for b in range(3):
+            v = vs.materialize_view(g, src[b], int(hop), int(rd))
+            np.testing.assert_array_equal(v.row_ptrs, z[f"rp_{c}_{b}"])
+            np.testing.assert_array_equal(v.cols, z[f"ci_{c}_{b}"])
+
+
 def test_view_capacity_error(vs):
     g = complete_graph(vs, 6)
     L = vs.capi.lib()

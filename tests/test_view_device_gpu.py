@@ -40,6 +40,24 @@ def test_device_halo_equals_host(vs, graphs, name):
                 _same(e.read_view(), vs.materialize_view(g, src, hop, root_degree))
 
 
+def test_device_halo_matches_reference_golden(vs):
+    """Device-built views equal the reference's ViewBin::Materialize output
+    (tests/golden/ref_views.npz, made from the reference sources)."""
+    import os
+    from conftest import ROOT
+    z = np.load(os.path.join(ROOT, "tests", "golden", "ref_views.npz"))
+    g = vs.Graph(z["row_ptrs"], z["cols"])
+    src = vs.sources_of_bins(z["bins"], 3)
+    with vs.Engine(g.V, [vs.plan_clique(3)]) as e:
+        e.upload_graph(g)
+        for c, (hop, rd) in enumerate(z["cases"]):
+            for b in range(3):
+                e.materialize_view(src[b], int(hop), int(rd))
+                v = e.read_view()
+                np.testing.assert_array_equal(v.row_ptrs, z[f"rp_{c}_{b}"])
+                np.testing.assert_array_equal(v.cols, z[f"ci_{c}_{b}"])
+
+
 def test_device_halo_edge_cases(vs, graphs):
     g = graphs["rmat8"]
     with vs.Engine(g.V, [vs.plan_clique(3)]) as e:
