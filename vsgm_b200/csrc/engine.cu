@@ -99,6 +99,9 @@ struct vsgm_engine {
   uint64_t* g_rp = nullptr;
   uint32_t* g_ci = nullptr;
   uint64_t g_cols = 0;
+  // per view: offset of each vertex's first larger neighbour (fused tails with a "> child" condition)
+  uint32_t* d_up = nullptr;
+  const uint64_t* up_of = nullptr;  // the row_ptrs d_up was computed for
 
   Arena arena;
   unsigned long long* d_counts = nullptr;  // [n_plans]
@@ -117,6 +120,7 @@ struct vsgm_engine {
     bool c4_aggregate = true;        // 4-cycle plans: wedge aggregation instead of the op sequence
     bool set_reuse = true;           // COMPUTE o + COMPUTE_COUNT w over the same set: count pairs of one intersection
     uint64_t c4_heavy = 1ull << 20;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
+    uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -153,6 +157,16 @@ struct vsgm_engine {
     uint64_t blocks = (work_items + 255) / 256;
     uint64_t cap = (uint64_t)sms * 16;
     return (unsigned)std::max<uint64_t>(1, std::min(blocks, cap));
+  }
+
+  const uint32_t* upper_offsets() {
+    if (up_of != d_rp || !d_up) {
+      if (!d_up) CK(cudaMalloc(&d_up, sizeof(uint32_t) * std::max<uint64_t>(V, 1)));
+      k_upper_offsets<<<grid_threads(V), 256, 0, stream>>>(d_rp, d_ci, V, d_up);
+      CK(cudaGetLastError());
+      up_of = d_rp;
+    }
+    return d_up;
   }
 
   uint64_t read_u64(const uint64_t* d) {
@@ -564,6 +578,8 @@ struct vsgm_engine {
     }
     fd.u = (uint8_t)u;
     fd.stage_cap = cur.stage_cap;
+    fd.walk_ratio = cur.walk_ratio;
+    fd.up = (fd.has_cond_u && fd.cond_u_op == VSGM_LARGER_THAN) ? upper_offsets() : nullptr;
     fd.other = -1;
     const vsgm_vgroup& cu = p.computed_unmat[i + 1];
     if (cu.count == 1) {
@@ -1064,6 +1080,7 @@ int vsgm_transfer_view(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t*
     e->n_cols = n_cols;
     e->n_src = n_sources;
     e->have_view = true;
+    e->up_of = nullptr;  // a new view: the upper offsets are stale
   });
 }
 
@@ -1075,6 +1092,7 @@ int vsgm_bind_view_device(vsgm_engine* e, const uint64_t* d_row_ptrs, const uint
   e->n_cols = n_cols;
   e->n_src = n_sources;
   e->have_view = true;
+  e->up_of = nullptr;
   return VSGM_OK;
 }
 
@@ -1152,6 +1170,7 @@ int vsgm_materialize_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_so
     e->n_cols = total;
     e->n_src = n_sources;
     e->have_view = true;
+    e->up_of = nullptr;  // a new view: the upper offsets are stale
   });
 }
 
@@ -1176,6 +1195,7 @@ int vsgm_graph_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_sources)
     e->n_cols = e->g_cols;
     e->n_src = n_sources;
     e->have_view = true;
+    e->up_of = nullptr;  // a new view: the upper offsets are stale
   });
 }
 
@@ -1257,6 +1277,11 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   }
   if (n == "c4_aggregate") {
     for (int k = lo; k < hi; k++) e->knobs[k].c4_aggregate = value != 0;
+    return VSGM_OK;
+  }
+  if (n == "walk_ratio") {
+    if (value < 0 || value > 65535) return engine_fail(e, VSGM_EINVAL, "walk_ratio must be 0..65535");
+    for (int k = lo; k < hi; k++) e->knobs[k].walk_ratio = (uint32_t)value;
     return VSGM_OK;
   }
   if (n == "c4_heavy") {
@@ -1369,6 +1394,7 @@ int vsgm_destroy(vsgm_engine* e) {
   cudaFree(e->own_src);
   cudaFree(e->g_rp);
   cudaFree(e->g_ci);
+  cudaFree(e->d_up);
   for (auto& r : e->rviews) {
     cudaFree(r.rp);
     cudaFree(r.ci);

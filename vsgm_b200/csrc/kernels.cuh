@@ -540,7 +540,17 @@ struct FusedDesc {
   int8_t other;        // computed vertex counted against (-1 none)
   uint8_t other_op;
   uint32_t stage_cap;  // <= kStageCap; smaller values force the per-child path
+  uint32_t walk_ratio; // a heavy child walks N(c) (probing the stage) unless N(c)'s part is this many times longer
+  const uint32_t* up;  // per vertex c: offset of the first neighbour > c in N(c) (cond_u_op LARGER_THAN), else null
 };
+
+// up[v] = index (within N(v)) of the first neighbour larger than v
+__global__ void k_upper_offsets(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint64_t V, uint32_t* __restrict__ up) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v < V; v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t a = rp[v];
+    up[v] = (uint32_t)(lower_bound(ci, a, rp[v + 1], v + 1) - a);
+  }
+}
 
 __device__ __forceinline__ uint32_t smem_lower_bound(const uint32_t* a, uint32_t lo, uint32_t hi, uint64_t x) {
   while (lo < hi) {
@@ -566,7 +576,7 @@ __device__ __forceinline__ void child_slice(const FusedDesc& fd, const Window& w
 }
 
 template <int NK, bool kOther>
-__global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+__global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
                                                    unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
   __shared__ uint32_t stage[8][kStageCap];
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
@@ -633,7 +643,7 @@ __global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const 
           } else if (ia < ib) {
             const uint64_t a0 = __ldg(rp + c), z0 = __ldg(rp + c + 1);
             const uint32_t excl = excl_child ? c : 0xffffffffu;
-            uint64_t cur = a0, ocur = 0;
+            uint64_t cur = fd.up ? a0 + __ldg(fd.up + c) : a0, ocur = 0;  // the slice lies above c
             acc_bytes += 4ull * (ib - ia) + 16ull;
             for (uint32_t j = ia; j < ib; j++) {
               const uint32_t x = I[j];
@@ -652,13 +662,14 @@ __global__ void __launch_bounds__(256) k_mat_count(Frame f, FusedDesc fd, const 
           uint32_t ia, ib;
           child_slice(fd, w, I, ni, c, &ia, &ib);
           const uint64_t a0 = __ldg(rp + c), z0 = __ldg(rp + c + 1);
-          const uint64_t s2 = warp_lower_bound(ci, a0, z0, I[ia]);
+          const uint64_t s2 = warp_lower_bound(ci, fd.up ? a0 + __ldg(fd.up + c) : a0, z0, I[ia]);
           const uint64_t e2 = warp_lower_bound(ci, s2, z0, (uint64_t)I[ib - 1] + 1);
           if (lane == 0) acc_bytes += 4ull * ((uint64_t)(ib - ia) < e2 - s2 ? (uint64_t)(ib - ia) : e2 - s2) + 16ull;
           if (s2 >= e2) continue;
           const uint32_t excl = excl_child ? c : 0xffffffffu;
           uint64_t ocur = 0;
-          if ((uint64_t)(ib - ia) <= (e2 - s2)) {
+          // walk N(c)'s part coalesced, probing the stage, unless it is much longer than the slice
+          if ((uint64_t)(ib - ia) * fd.walk_ratio < (e2 - s2)) {
             uint64_t cur = s2;
             for (uint32_t j = ia + lane; j < ib; j += kWarp) {
               const uint32_t x = I[j];
