@@ -224,6 +224,10 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   rooted at each cycle's largest vertex (sum over opposite vertices of
  *   C(wedges, 2)) instead of the plan's op sequence; totals are identical, per-view
  *   counts are attributed to the largest instead of the smallest vertex;
+ *   "walk_ratio" (default 8): in the fused tail a child with a long slice of the
+ *   staged set walks its own adjacency range coalesced (probing the stage) unless
+ *   that range is this many times longer than the slice, then it gallops (0: always
+ *   gallop);
  *   "c4_heavy" (default 2^20): roots with at least this many wedges are counted by
  *   groups sharing the whole GPU with L2-resident counters (0: every root);
  *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT

@@ -278,6 +278,11 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
                 e.reset_counts()
                 e.match()
                 assert e.counts() == want, (ratio, lane)
+        for walk in (0, 1, 8, 1000):
+            e.set_option("walk_ratio", walk)
+            e.reset_counts()
+            e.match()
+            assert e.counts() == want, walk
         report = autotune(e, len(plans), stride=4)
         assert [r["plan"] for r in report] == list(range(len(plans)))
         e.match()

@@ -1,7 +1,7 @@
 """Autotuner for the engine's per-plan knobs (intersection variant and tail fusion).
 
-For every plan it times each candidate setting of (fuse_tail, merge_ratio,
-lane_merge, stage_cap) on a strided sample of the view's roots (engine option root_stride)
+For every plan it times each candidate setting of (c4_aggregate, fuse_tail,
+merge_ratio, lane_merge, stage_cap, walk_ratio) on a strided sample of the view's roots (engine option root_stride)
 and keeps the fastest; the choice is written back as per-plan options.  Counts
 never depend on these knobs, so tuning on a sample is safe; the sample only has
 to rank the settings.
@@ -15,6 +15,7 @@ CANDIDATES = {
     "merge_ratio": (0, 4, 16),
     "lane_merge": (0, 1),
     "stage_cap": (1536, 384),
+    "walk_ratio": (8, 1),
 }
 
 
@@ -22,12 +23,13 @@ def _settings(space):
     keys = list(space)
     for vals in itertools.product(*(space[k] for k in keys)):
         cfg = dict(zip(keys, vals))
-        if not cfg["fuse_tail"] and cfg["stage_cap"] != space["stage_cap"][0]:
-            continue  # the stage only matters for the fused tail
+        if not cfg["fuse_tail"] and (cfg["stage_cap"] != space["stage_cap"][0] or cfg.get("walk_ratio", 0) != space.get("walk_ratio", (0,))[0]):
+            continue  # the stage and the walk only matter for the fused tail
         if cfg.get("lane_merge") and not cfg["merge_ratio"]:
             continue  # no merge, nothing to partition
         if cfg.get("c4_aggregate") and (cfg["fuse_tail"] != space["fuse_tail"][0] or cfg["merge_ratio"] != space["merge_ratio"][0]
-                                        or cfg.get("lane_merge") or cfg["stage_cap"] != space["stage_cap"][0]):
+                                        or cfg.get("lane_merge") or cfg["stage_cap"] != space["stage_cap"][0]
+                                        or cfg.get("walk_ratio", 0) != space.get("walk_ratio", (0,))[0]):
             continue  # the other knobs do not matter when a 4-cycle is aggregated
         yield cfg
 
