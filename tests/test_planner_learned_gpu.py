@@ -47,9 +47,10 @@ def test_held_out_work_not_above_heuristic(setup):
         order, took = model.choose_verified(base, sampler, vi, k=4)
         used += took
         plans = [lp.plan_reorder(base, lp.heuristic_order(base)), lp.plan_reorder(base, order)]
+        # a different order roots each match at a different pattern vertex, so the
+        # counts of one root sample differ; the work on a uniform root sample is an
+        # unbiased estimate of each order's whole-view work
         cnt, lvl, ovf = check.evaluate(plans, vi)
-        if not ovf.any():
-            assert cnt[0][0] == cnt[1][0]  # same sampled roots, same exact count
         w = [sum(int(x) for x in lvl[i][0][:plans[i].n_ops]) for i in range(2)]
         heur += w[0]
         learned += w[1]

@@ -1434,7 +1434,10 @@ constexpr size_t kNoAllocDescOff = 256;
 constexpr size_t kNoAllocTaskOff = 1280;
 constexpr size_t kNoAllocScratchOff = (kNoAllocTaskOff + kNoAllocMaxTasks * sizeof(DfsTask) + 255) & ~(size_t)255;
 constexpr uint64_t kNoAllocWarpU32 = (kNoAllocBytes - kNoAllocScratchOff) / (kNoAllocWarps * sizeof(uint32_t));
-static_assert(sizeof(DfsPlan) + sizeof(DfsView) <= kNoAllocTaskOff - kNoAllocDescOff, "plan + view must fit their slot");
+// the view descriptor (8-byte pointers) follows the plan at the next 16-byte boundary
+constexpr size_t kNoAllocViewOff = kNoAllocDescOff + ((sizeof(DfsPlan) + 15) & ~(size_t)15);
+static_assert(kNoAllocViewOff % alignof(DfsView) == 0 && kNoAllocTaskOff % alignof(DfsTask) == 0, "descriptor alignment");
+static_assert(kNoAllocViewOff + sizeof(DfsView) <= kNoAllocTaskOff, "plan + view must fit their slot");
 static_assert(kNoAllocWarpU32 == 24319, "the documented limit (plan ops x max degree) follows the layout");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -1498,7 +1501,7 @@ extern "C" int vsgm_count_noalloc(int device, const vsgm_plan* plan, uint64_t V,
     }
     NoAllocCounters* ctr = (NoAllocCounters*)base;
     DfsPlan* d_plan = (DfsPlan*)(base + kNoAllocDescOff);
-    DfsView* d_view = (DfsView*)(base + kNoAllocDescOff + sizeof(DfsPlan));
+    DfsView* d_view = (DfsView*)(base + kNoAllocViewOff);
     DfsTask* d_tasks = (DfsTask*)(base + kNoAllocTaskOff);
     uint32_t* scratch = (uint32_t*)(base + kNoAllocScratchOff);
     // the array keeps the previous call's contents: clear the counters

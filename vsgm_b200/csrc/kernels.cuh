@@ -805,6 +805,37 @@ __global__ void k_expand(Frame in, Expand x, const uint64_t* __restrict__ off, u
 }
 
 // ---------------------------------------------------------------------------
+// Load-balanced walk over up to 32 short rows at once: lane l owns the range
+// [a_l, a_l + n_l) of ci (n_l = 0 for no row); every round the 32 lanes read 32
+// consecutive entries of the concatenated ranges (owner found by a 5-step search
+// over the inclusive prefix of n), so the loads of a warp are independent instead
+// of one row's chain at a time.  f(owner's tag, entry value) is called per entry.
+// ---------------------------------------------------------------------------
+template <typename F>
+__device__ __forceinline__ void warp_rows(uint64_t a, uint64_t n, uint32_t tag, const uint32_t* __restrict__ ci, F&& f) {
+  const unsigned lane = lane_id();
+  uint64_t inc = n;
+#pragma unroll
+  for (int o = 1; o < kWarp; o <<= 1) {
+    const uint64_t t = __shfl_up_sync(kFull, inc, o);
+    if (lane >= (unsigned)o) inc += t;
+  }
+  const uint64_t total = __shfl_sync(kFull, inc, kWarp - 1);
+  const uint64_t excl = inc - n;
+  for (uint64_t base = 0; base < total; base += kWarp) {
+    const uint64_t t = base + lane;
+    unsigned lo = 0;  // lanes whose inclusive prefix is <= t (the prefix is non-decreasing)
+#pragma unroll
+    for (unsigned step = 16; step > 0; step >>= 1)
+      if (__shfl_sync(kFull, inc, lo + step - 1) <= t) lo += step;
+    const unsigned owner = lo < kWarp ? lo : kWarp - 1;
+    const uint64_t oa = __shfl_sync(kFull, a, owner), oe = __shfl_sync(kFull, excl, owner);
+    const uint32_t otag = __shfl_sync(kFull, tag, owner);
+    if (t < total) f(otag, __ldg(ci + oa + (t - oe)));
+  }
+}
+
+// ---------------------------------------------------------------------------
 // 4-cycle count by wedge aggregation.  Every 4-cycle is counted once, at its
 // largest vertex u: for each neighbour v < u and each w in N(v) with w < u,
 // L[w] counts the wedges u-v-w; the cycles closed at u are sum C(L[w], 2)
@@ -833,17 +864,21 @@ __global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict
     const unsigned long long r = s_root;
     if (r >= n_roots) break;
     const uint32_t u = __ldg(roots + r);
-    const uint64_t ua = __ldg(rp + u), uz = __ldg(rp + u + 1);
-    // wedges: warp per neighbour v < u, lanes over N(v) below u
-    for (uint64_t k = ua + warp; k < uz; k += nwarps) {
-      const uint32_t v = __ldg(ci + k);
-      if (v >= u) break;  // rows are sorted
-      const uint64_t va = __ldg(rp + v), vz = __ldg(rp + v + 1);
-      for (uint64_t j = va + lane; j < vz; j += kWarp) {
-        const uint32_t w = __ldg(ci + j);
-        if (w >= u) break;
-        if (atomicAdd(L + w, 1u) == 0u) touched[atomicAdd(&s_touched, 1u)] = w;
+    const uint64_t ua = __ldg(rp + u);
+    const uint64_t ub = lower_bound(ci, ua, __ldg(rp + u + 1), u);  // centres v < u
+    // wedges: each warp takes 32 centres at a time, one per lane, and walks their
+    // rows below u together
+    for (uint64_t k0 = ua + (uint64_t)warp * kWarp; k0 < ub; k0 += (uint64_t)nwarps * kWarp) {
+      const uint64_t k = k0 + lane;
+      uint64_t va = 0, vn = 0;
+      if (k < ub) {
+        const uint32_t v = __ldg(ci + k);
+        va = __ldg(rp + v);
+        vn = lower_bound(ci, va, __ldg(rp + v + 1), u) - va;
       }
+      warp_rows(va, vn, 0u, ci, [&](uint32_t, uint32_t w) {
+        if (atomicAdd(L + w, 1u) == 0u) touched[atomicAdd(&s_touched, 1u)] = w;
+      });
     }
     __syncthreads();
     const unsigned n = s_touched;
@@ -916,19 +951,20 @@ __global__ void __launch_bounds__(256) k_c4_group_wedges(const uint64_t* __restr
   const uint64_t total = G.vbeg[G.n];
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
   const unsigned lane = lane_id();
-  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < total; i += warps) {
+  // each warp takes 32 centres at a time (one per lane, possibly of different
+  // roots of the group) and walks their rows below their roots together
+  for (uint64_t i0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp * kWarp; i0 < total; i0 += warps * kWarp) {
+    const uint64_t i = i0 + lane;
+    uint64_t va = 0, vn = 0;
     uint32_t g = 0;
-    while (g + 1 < G.n && i >= G.vbeg[g + 1]) g++;
-    const uint32_t u = G.root[g];
-    const uint32_t v = __ldg(ci + __ldg(rp + u) + (i - G.vbeg[g]));  // v < u: the row is sorted
-    uint32_t* Lg = L + (uint64_t)g * stride;
-    const uint64_t z = __ldg(rp + v + 1);
-    for (uint64_t base = __ldg(rp + v); base < z; base += kWarp) {
-      const uint64_t j = base + lane;
-      const uint32_t w = j < z ? __ldg(ci + j) : u;
-      if (w < u) atomicAdd(Lg + w, 1u);
-      if (__any_sync(kFull, w >= u)) break;
+    if (i < total) {
+      while (g + 1 < G.n && i >= G.vbeg[g + 1]) g++;
+      const uint32_t u = G.root[g];
+      const uint32_t v = __ldg(ci + __ldg(rp + u) + (i - G.vbeg[g]));  // v < u: the row is sorted
+      va = __ldg(rp + v);
+      vn = lower_bound(ci, va, __ldg(rp + v + 1), u) - va;
     }
+    warp_rows(va, vn, g, ci, [&](uint32_t og, uint32_t w) { atomicAdd(L + (uint64_t)og * stride + w, 1u); });
   }
 }
 
