@@ -10,8 +10,8 @@ A step is one match of all three queries over the resident view.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--scale S] [--queries kc4,p1,p2] [--option knob=value ...]
 
-(--scale / --queries / --option select smaller or single-query cases for
-profiling; the default is the workload above.)
+(--scale / --queries / --option / --hbm-gb select smaller or single-query cases
+for profiling; the default is the workload above.)
 
 value   = sum of the exact counts / device time per step (inputs resident in HBM)
 e2e     = the same through the C ABI from pinned host buffers: view upload +
@@ -185,6 +185,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--queries", default="kc4,p1,p2", help="comma list of kcK / pN (default: the workload's three)")
     ap.add_argument("--option", action="append", default=[], help="engine knob name=value (vsgm_set_option), repeatable")
+    ap.add_argument("--hbm-gb", type=float, default=0.0,
+                    help="engine working budget in GB (0: 90%% of free HBM); profiler captures use a few GB")
     args = ap.parse_args()
     args.query_flags = parse_queries(args.queries)
     if args.query_flags != WORKLOAD["queries"] or args.scale != 22:
@@ -210,7 +212,7 @@ def main():
     # roots of this rank: a strided share of the vertices (one view per rank)
     from vsgm_b200.shard import allreduce_counts, roots_of_rank
     roots = roots_of_rank(g.V, rank, world)
-    eng = vs.Engine(g.V, plans, device=local)
+    eng = vs.Engine(g.V, plans, device=local, hbm_budget_bytes=int(args.hbm_gb * 1e9))
     stream = torch.cuda.ExternalStream(eng.stream(), device=local)
     for kv in args.option:
         name, val = kv.split("=")
