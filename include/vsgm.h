@@ -189,6 +189,7 @@ typedef struct vsgm_batch_stats {
   uint64_t launches;      /* kernels launched by it */
   uint64_t scratch_bytes; /* per-warp scratch allocated */
   double ms;              /* device time (with profiling on) */
+  uint64_t level_pairs;   /* (plan, view) pairs the hybrid run counted level-wise */
 } vsgm_batch_stats;
 int vsgm_get_batch_stats(vsgm_engine* e, vsgm_batch_stats* out);
 
@@ -235,6 +236,10 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   counts the pairs of one intersection instead of intersecting twice;
  *   "lane_merge" (default 0): counting kernels merge two such lists with each lane
  *   walking its own chunk instead of 32-element warp windows;
+ *   "hybrid_steps" (engine-wide, default 2^17): vsgm_run_batched runs every pair in
+ *   the persistent launch with this per-task step bound and counts the pairs it
+ *   stopped again with the level-wise engine on their resident view (0: the
+ *   persistent launch alone, unbounded);
  *   "root_stride" (engine-wide, default 1): match only every k-th source of the view
  *   (the autotuner's samples; counts are then those of the sample);
  *   "only_plan" (engine-wide, default -1): vsgm_match runs only this plan.

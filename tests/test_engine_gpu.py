@@ -146,9 +146,17 @@ def test_batched_persistent_run_matches_oracle(vs, orc, graphs):
     V = max(g.V for g in views)
     with vs.Engine(V, plans) as e:
         ids = [e.add_view(g) for g in views]
+        e.set_option("hybrid_steps", 0)  # the persistent launch alone
         got = e.run_batched(ids)
         st = e.batch_stats()
-        assert st.launches == 1 and st.tasks >= len(plans) * len(views)
+        assert st.launches == 1 and st.tasks >= len(plans) * len(views) and st.level_pairs == 0
+        # hybrid: pairs whose tasks exceed the step bound are counted level-wise
+        e.set_option("hybrid_steps", 1)
+        every = e.run_batched(ids)
+        assert e.batch_stats().level_pairs == len(plans) * len(views)
+        e.set_option("hybrid_steps", 1 << 17)
+        default = e.run_batched(ids)
+    assert every == got and default == got
     for pi, (name, p) in enumerate(named):
         want = [orc.count(p, g) for g in views]
         assert got[pi] == want, (name, p.describe())

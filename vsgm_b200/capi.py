@@ -85,7 +85,8 @@ class Plan(C.Structure):
 
 
 class BatchStats(C.Structure):
-    _fields_ = [("tasks", C.c_uint64), ("launches", C.c_uint64), ("scratch_bytes", C.c_uint64), ("ms", C.c_double)]
+    _fields_ = [("tasks", C.c_uint64), ("launches", C.c_uint64), ("scratch_bytes", C.c_uint64), ("ms", C.c_double),
+                ("level_pairs", C.c_uint64)]
 
 
 class PlanStats(C.Structure):

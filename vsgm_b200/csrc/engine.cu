@@ -102,6 +102,7 @@ struct vsgm_engine {
   // per view: offset of each vertex's first larger neighbour (fused tails with a "> child" condition)
   uint32_t* d_up = nullptr;
   const uint64_t* up_of = nullptr;  // the row_ptrs d_up was computed for
+  uint64_t up_cap = 0;
 
   Arena arena;
   unsigned long long* d_counts = nullptr;  // [n_plans]
@@ -125,8 +126,10 @@ struct vsgm_engine {
   std::vector<Knobs> knobs;
   Knobs cur;
   uint64_t root_stride = 1;  // >1: match only every root_stride-th source (autotuning samples)
+  uint64_t hybrid_steps = 1ull << 17;  // vsgm_run_batched: pairs whose tasks exceed this many steps rerun level-wise (0: never)
   int only_plan = -1;        // >=0: vsgm_match runs this plan only
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_h0 = nullptr, ev_h1 = nullptr;  // around a hybrid batched run
   std::string err;
 
   // resident views for batched runs (vsgm_add_view)
@@ -161,7 +164,14 @@ struct vsgm_engine {
 
   const uint32_t* upper_offsets() {
     if (up_of != d_rp || !d_up) {
-      if (!d_up) CK(cudaMalloc(&d_up, sizeof(uint32_t) * std::max<uint64_t>(V, 1)));
+      if (d_up && up_cap < V) {
+        CK(cudaFree(d_up));
+        d_up = nullptr;
+      }
+      if (!d_up) {
+        CK(cudaMalloc(&d_up, sizeof(uint32_t) * std::max<uint64_t>(V, 1)));
+        up_cap = V;
+      }
       k_upper_offsets<<<grid_threads(V), 256, 0, stream>>>(d_rp, d_ci, V, d_up);
       CK(cudaGetLastError());
       up_of = d_rp;
@@ -929,6 +939,7 @@ struct vsgm_engine {
     if ((uint32_t)hc[(uint64_t)n_plans * n_views + 1] != 0) throw OutOfMemory{"batched run: a candidate set exceeded the per-warp scratch"};
     bstats.tasks = ht.size();
     bstats.launches = 1;
+    bstats.level_pairs = 0;
     bstats.scratch_bytes = grid * kDfsWarps * levels * cap * 4;
     bstats.ms = 0;
     if (profiling) {
@@ -939,6 +950,51 @@ struct vsgm_engine {
     for (uint64_t k = 0; k < (uint64_t)n_plans * n_views; k++) out[k] = hc[k];
     if (level_out) CK(cudaMemcpy(level_out, d_lvl, sizeof(uint64_t) * pairs * VSGM_MAX_OPS, cudaMemcpyDeviceToHost));
     if (overflow_out) CK(cudaMemcpy(overflow_out, d_ovf, sizeof(uint32_t) * pairs, cudaMemcpyDeviceToHost));
+  }
+
+  // The level-wise engine on one resident view (the hybrid batched run's heavy
+  // pairs): the view temporarily becomes the current one.
+  uint64_t run_resident(int vid, int pk) {
+    const ResidentView& r = rviews[vid];
+    const uint64_t* s_rp = d_rp;
+    const uint32_t* s_ci = d_ci;
+    const uint32_t* s_src = d_src;
+    const uint64_t s_nsrc = n_src, s_ncols = n_cols, s_V = V, s_stride = root_stride;
+    root_stride = 1;  // every source of the view, as the persistent launch does
+    d_rp = r.rp;
+    d_ci = r.ci;
+    d_src = r.src;
+    n_src = r.n_src;
+    n_cols = r.n_cols;
+    V = r.V;
+    up_of = nullptr;
+    uint64_t c = 0;
+    try {
+      CK(cudaMemsetAsync(d_counts + pk, 0, sizeof(unsigned long long), stream));
+      stats[pk] = vsgm_plan_stats{};
+      arena.top = 0;
+      run_plan(pk);
+      c = read_u64((const uint64_t*)(d_counts + pk));
+    } catch (...) {
+      d_rp = const_cast<uint64_t*>(s_rp);
+      d_ci = const_cast<uint32_t*>(s_ci);
+      d_src = const_cast<uint32_t*>(s_src);
+      n_src = s_nsrc;
+      n_cols = s_ncols;
+      V = s_V;
+      root_stride = s_stride;
+      up_of = nullptr;
+      throw;
+    }
+    d_rp = const_cast<uint64_t*>(s_rp);
+    d_ci = const_cast<uint32_t*>(s_ci);
+    d_src = const_cast<uint32_t*>(s_src);
+    n_src = s_nsrc;
+    n_cols = s_ncols;
+    V = s_V;
+    root_stride = s_stride;
+    up_of = nullptr;
+    return c;
   }
 
   void run_plan(int pi) {
@@ -1027,6 +1083,8 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&e->ev0));
     CK(cudaEventCreate(&e->ev1));
+    CK(cudaEventCreate(&e->ev_h0));
+    CK(cudaEventCreate(&e->ev_h1));
     CK(cudaMalloc(&e->d_counts, sizeof(unsigned long long) * (n_plans + 2)));
     e->d_bytes = e->d_counts + n_plans;
     CK(cudaMemset(e->d_counts, 0, sizeof(unsigned long long) * (n_plans + 2)));
@@ -1303,6 +1361,11 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
     e->only_plan = (int)value;
     return VSGM_OK;
   }
+  if (n == "hybrid_steps") {
+    if (value < 0) return engine_fail(e, VSGM_EINVAL, "hybrid_steps must be >= 0");
+    e->hybrid_steps = (uint64_t)value;
+    return VSGM_OK;
+  }
   if (n == "root_stride") {
     if (value < 1) return engine_fail(e, VSGM_EINVAL, "root_stride must be >= 1");
     e->root_stride = (uint64_t)value;
@@ -1359,7 +1422,34 @@ int vsgm_run_batched(vsgm_engine* e, const int* view_ids, int n_views, const int
   return guarded(e, [&] {
     CK(cudaSetDevice(e->device));
     e->arena.top = 0;
-    e->run_batched(view_ids, n_views, plan_ids, n_plans, counts);
+    if (!e->hybrid_steps) {
+      e->run_batched(view_ids, n_views, plan_ids, n_plans, counts);
+      return;
+    }
+    // hybrid: one persistent launch finishes every pair whose tasks stay within the
+    // step bound; the pairs it stopped are counted again by the level-wise engine
+    // on their resident view (their partial counts are discarded)
+    if (e->profiling) CK(cudaEventRecord(e->ev_h0, e->stream));
+    std::vector<uint32_t> ovf((size_t)n_plans * n_views, 0);
+    e->run_batched(view_ids, n_views, plan_ids, n_plans, counts, nullptr, e->hybrid_steps, ovf.data());
+    vsgm_batch_stats bs = e->bstats;
+    for (int p = 0; p < n_plans; p++)
+      for (int v = 0; v < n_views; v++) {
+        const size_t k = (size_t)p * n_views + v;
+        if (!ovf[k]) continue;
+        counts[k] = e->run_resident(view_ids[v], plan_ids[p]);
+        const vsgm_plan_stats& st = e->stats[plan_ids[p]];
+        for (uint32_t i = 0; i < e->plans[plan_ids[p]].n_ops; i++) bs.launches += st.op_launches[i];
+        bs.level_pairs++;
+      }
+    if (e->profiling) {
+      CK(cudaEventRecord(e->ev_h1, e->stream));
+      CK(cudaEventSynchronize(e->ev_h1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, e->ev_h0, e->ev_h1));
+      bs.ms = ms;
+    }
+    e->bstats = bs;
   });
 }
 
@@ -1403,6 +1493,8 @@ int vsgm_destroy(vsgm_engine* e) {
   if (e->h_pinned) cudaFreeHost(e->h_pinned);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->ev_h0) cudaEventDestroy(e->ev_h0);
+  if (e->ev_h1) cudaEventDestroy(e->ev_h1);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return VSGM_OK;
