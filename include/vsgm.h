@@ -177,6 +177,10 @@ int vsgm_add_view(vsgm_engine* e, uint64_t V, const uint64_t* row_ptrs, const ui
                   uint64_t n_sources, int* view_id);
 int vsgm_run_batched(vsgm_engine* e, const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* counts);
 
+/* The same persistent (hybrid) run over an explicit list of (plan, view) pairs,
+ * e.g. a different plan of one pattern per view; counts[i] for pair i. */
+int vsgm_run_pairs(vsgm_engine* e, const int* plan_ids, const int* view_ids, int n_pairs, uint64_t* counts);
+
 /* vsgm_run_batched plus, per (plan, view) pair: level_paths[pair * VSGM_MAX_OPS + i]
  * = partial matches entering op i (the intermediate sizes the learned planner is
  * trained on), and with step_budget > 0 every task stops after that many steps and

@@ -156,6 +156,12 @@ def test_batched_persistent_run_matches_oracle(vs, orc, graphs):
         assert e.batch_stats().level_pairs == len(plans) * len(views)
         e.set_option("hybrid_steps", 1 << 17)
         default = e.run_batched(ids)
+        # an explicit pair list gives the same counts as the cross product
+        rng = np.random.default_rng(2)
+        pairs = [(int(a), int(b)) for a, b in zip(rng.integers(0, len(plans), 40), rng.integers(0, len(views), 40))]
+        for steps in (0, 1, 1 << 17):
+            e.set_option("hybrid_steps", steps)
+            assert e.run_pairs(pairs) == [got[a][b] for a, b in pairs], steps
     assert every == got and default == got
     for pi, (name, p) in enumerate(named):
         want = [orc.count(p, g) for g in views]

@@ -271,6 +271,15 @@ class Engine:
         capi.check(_L().vsgm_run_batched(self.h, v, len(view_ids), p, len(plan_ids), capi.ptr(out, C.c_uint64)), self.h)
         return [[int(x) for x in out[i * len(view_ids):(i + 1) * len(view_ids)]] for i in range(len(plan_ids))]
 
+    def run_pairs(self, pairs):
+        """Counts of an explicit list of (plan id, view id) pairs in one persistent run."""
+        n = len(pairs)
+        p = (C.c_int * n)(*[int(a) for a, _ in pairs])
+        v = (C.c_int * n)(*[int(b) for _, b in pairs])
+        out = np.zeros(n, np.uint64)
+        capi.check(_L().vsgm_run_pairs(self.h, p, v, n, capi.ptr(out, C.c_uint64)), self.h)
+        return [int(x) for x in out]
+
     def run_batched_ex(self, view_ids, plan_ids=None, step_budget=0):
         """Counts [plan][view], level paths [plan][view][op] and overflow flags [plan][view]."""
         plan_ids = list(range(len(self.plans))) if plan_ids is None else list(plan_ids)

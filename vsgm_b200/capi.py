@@ -145,6 +145,7 @@ _SIGS = {
     "vsgm_set_plan_option": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, C.c_int64]),
     "vsgm_add_view": (C.c_int, [C.c_void_p, C.c_uint64, _u64p, _u32p, C.c_uint64, _u32p, C.c_uint64, _P(C.c_int)]),
     "vsgm_run_batched": (C.c_int, [C.c_void_p, _P(C.c_int), C.c_int, _P(C.c_int), C.c_int, _u64p]),
+    "vsgm_run_pairs": (C.c_int, [C.c_void_p, _P(C.c_int), _P(C.c_int), C.c_int, _u64p]),
     "vsgm_get_batch_stats": (C.c_int, [C.c_void_p, _P(BatchStats)]),
     "vsgm_run_batched_ex": (C.c_int, [C.c_void_p, _P(C.c_int), C.c_int, _P(C.c_int), C.c_int, C.c_uint64, _u64p, _u64p, _u32p]),
     "vsgm_engine_stream": (C.c_void_p, [C.c_void_p]),

@@ -853,8 +853,10 @@ struct vsgm_engine {
 
   // One persistent launch over every (plan, view) pair: tasks are root ranges of
   // balanced estimated cost, longest first, popped by warps from a device queue.
+  // mask (optional): mask[plan * n_views + view] != 0 for the pairs to count; the
+  // others get no tasks and count 0
   void run_batched(const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* out, uint64_t* level_out = nullptr,
-                   uint64_t step_budget = 0, uint32_t* overflow_out = nullptr) {
+                   uint64_t step_budget = 0, uint32_t* overflow_out = nullptr, const uint8_t* mask = nullptr) {
     std::vector<DfsPlan> hp(n_plans);
     uint32_t levels = 1;
     for (int k = 0; k < n_plans; k++) {
@@ -880,6 +882,7 @@ struct vsgm_engine {
     const double target = std::max(1.0, total / (double)(warps * 16));
     for (int pk = 0; pk < n_plans; pk++)
       for (int k = 0; k < n_views; k++) {
+        if (mask && !mask[(size_t)pk * n_views + k]) continue;
         const auto& deg = rviews[view_ids[k]].h_deg_src;
         const bool splittable = hp[pk].split_lvl < hp[pk].n_ops;
         uint64_t r0 = 0;
@@ -950,6 +953,38 @@ struct vsgm_engine {
     for (uint64_t k = 0; k < (uint64_t)n_plans * n_views; k++) out[k] = hc[k];
     if (level_out) CK(cudaMemcpy(level_out, d_lvl, sizeof(uint64_t) * pairs * VSGM_MAX_OPS, cudaMemcpyDeviceToHost));
     if (overflow_out) CK(cudaMemcpy(overflow_out, d_ovf, sizeof(uint32_t) * pairs, cudaMemcpyDeviceToHost));
+  }
+
+  // Hybrid batched run (knob hybrid_steps): one persistent launch finishes every
+  // pair whose tasks stay within the step bound; the pairs it stopped are counted
+  // again by the level-wise engine on their resident view (their partial counts
+  // are discarded).
+  void run_hybrid(const int* view_ids, int n_views, const int* plan_ids, int n_plans, uint64_t* counts, const uint8_t* mask) {
+    if (!hybrid_steps) {
+      run_batched(view_ids, n_views, plan_ids, n_plans, counts, nullptr, 0, nullptr, mask);
+      return;
+    }
+    if (profiling) CK(cudaEventRecord(ev_h0, stream));
+    std::vector<uint32_t> ovf((size_t)n_plans * n_views, 0);
+    run_batched(view_ids, n_views, plan_ids, n_plans, counts, nullptr, hybrid_steps, ovf.data(), mask);
+    vsgm_batch_stats bs = bstats;
+    for (int p = 0; p < n_plans; p++)
+      for (int v = 0; v < n_views; v++) {
+        const size_t k = (size_t)p * n_views + v;
+        if (!ovf[k]) continue;
+        counts[k] = run_resident(view_ids[v], plan_ids[p]);
+        const vsgm_plan_stats& st = stats[plan_ids[p]];
+        for (uint32_t i = 0; i < plans[plan_ids[p]].n_ops; i++) bs.launches += st.op_launches[i];
+        bs.level_pairs++;
+      }
+    if (profiling) {
+      CK(cudaEventRecord(ev_h1, stream));
+      CK(cudaEventSynchronize(ev_h1));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, ev_h0, ev_h1));
+      bs.ms = ms;
+    }
+    bstats = bs;
   }
 
   // The level-wise engine on one resident view (the hybrid batched run's heavy
@@ -1422,34 +1457,35 @@ int vsgm_run_batched(vsgm_engine* e, const int* view_ids, int n_views, const int
   return guarded(e, [&] {
     CK(cudaSetDevice(e->device));
     e->arena.top = 0;
-    if (!e->hybrid_steps) {
-      e->run_batched(view_ids, n_views, plan_ids, n_plans, counts);
-      return;
+    e->run_hybrid(view_ids, n_views, plan_ids, n_plans, counts, nullptr);
+  });
+}
+
+int vsgm_run_pairs(vsgm_engine* e, const int* plan_ids, const int* view_ids, int n_pairs, uint64_t* counts) {
+  if (!e || !view_ids || !plan_ids || !counts || n_pairs < 1) return engine_fail(e, VSGM_EINVAL, "bad pairs request");
+  for (int k = 0; k < n_pairs; k++) {
+    if (view_ids[k] < 0 || view_ids[k] >= (int)e->rviews.size()) return engine_fail(e, VSGM_EINVAL, "unknown view id");
+    if (plan_ids[k] < 0 || plan_ids[k] >= (int)e->plans.size()) return engine_fail(e, VSGM_EINVAL, "unknown plan id");
+  }
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    e->arena.top = 0;
+    // the distinct plans and views, and the mask of the requested pairs
+    std::vector<int> P, W;
+    std::vector<int> pi(n_pairs), wi(n_pairs);
+    for (int k = 0; k < n_pairs; k++) {
+      auto fp = std::find(P.begin(), P.end(), plan_ids[k]);
+      pi[k] = (int)(fp - P.begin());
+      if (fp == P.end()) P.push_back(plan_ids[k]);
+      auto fw = std::find(W.begin(), W.end(), view_ids[k]);
+      wi[k] = (int)(fw - W.begin());
+      if (fw == W.end()) W.push_back(view_ids[k]);
     }
-    // hybrid: one persistent launch finishes every pair whose tasks stay within the
-    // step bound; the pairs it stopped are counted again by the level-wise engine
-    // on their resident view (their partial counts are discarded)
-    if (e->profiling) CK(cudaEventRecord(e->ev_h0, e->stream));
-    std::vector<uint32_t> ovf((size_t)n_plans * n_views, 0);
-    e->run_batched(view_ids, n_views, plan_ids, n_plans, counts, nullptr, e->hybrid_steps, ovf.data());
-    vsgm_batch_stats bs = e->bstats;
-    for (int p = 0; p < n_plans; p++)
-      for (int v = 0; v < n_views; v++) {
-        const size_t k = (size_t)p * n_views + v;
-        if (!ovf[k]) continue;
-        counts[k] = e->run_resident(view_ids[v], plan_ids[p]);
-        const vsgm_plan_stats& st = e->stats[plan_ids[p]];
-        for (uint32_t i = 0; i < e->plans[plan_ids[p]].n_ops; i++) bs.launches += st.op_launches[i];
-        bs.level_pairs++;
-      }
-    if (e->profiling) {
-      CK(cudaEventRecord(e->ev_h1, e->stream));
-      CK(cudaEventSynchronize(e->ev_h1));
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, e->ev_h0, e->ev_h1));
-      bs.ms = ms;
-    }
-    e->bstats = bs;
+    std::vector<uint8_t> mask(P.size() * W.size(), 0);
+    for (int k = 0; k < n_pairs; k++) mask[(size_t)pi[k] * W.size() + wi[k]] = 1;
+    std::vector<uint64_t> all(P.size() * W.size(), 0);
+    e->run_hybrid(W.data(), (int)W.size(), P.data(), (int)P.size(), all.data(), mask.data());
+    for (int k = 0; k < n_pairs; k++) counts[k] = all[(size_t)pi[k] * W.size() + wi[k]];
   });
 }
 
