@@ -193,6 +193,19 @@ class LearnedPlanner:
             losses.append(loss.value)
         return losses
 
+    def save(self, path):
+        """Write the FP32 master parameters (packed as the C ABI packs them) to a .npy file."""
+        n = int(self.L.vsgm_mlp_num_params(self.h))
+        w = np.zeros(n, np.float32)
+        capi.check(self.L.vsgm_mlp_get_params(self.h, self._p(w)))
+        np.save(path, w)
+
+    def load(self, path):
+        w = np.ascontiguousarray(np.load(path), np.float32)
+        if w.size != int(self.L.vsgm_mlp_num_params(self.h)):
+            raise ValueError("parameter file does not match the network's shape")
+        capi.check(self.L.vsgm_mlp_set_params(self.h, self._p(w)))
+
     def predict(self, X):
         X = np.ascontiguousarray(X, np.float32)
         y = np.zeros((len(X), N_OUT), np.float32)
@@ -225,6 +238,31 @@ class LearnedPlanner:
         if best != 0 and work[best] < (1.0 - margin) * work[0]:
             return cands[best], True
         return h, False
+
+    def choose_verified_many(self, plans, sampler, view_index, k=4, margin=0.05):
+        """choose_verified for many patterns on one view with two sampled runs in
+        total (features of every heuristic plan, then every pattern's candidates)."""
+        hs = [heuristic_order(p) for p in plans]
+        _, lvl0, _ = sampler.evaluate(list(plans), view_index)
+        X = np.stack([features(p, sampler.hist[view_index], lvl0[i][0]) for i, p in enumerate(plans)])
+        pred = self.predict(X)
+        cands, owner = [], []
+        for i, p in enumerate(plans):
+            ranked = sorted((o for o in valid_orders(p) if o != hs[i]), key=lambda o: pred[i][order_index(o)])
+            for o in [hs[i]] + ranked[:k]:
+                cands.append(plan_reorder(p, o))
+                owner.append((i, o))
+        _, lvl, ovf = sampler.evaluate(cands, view_index)
+        best = {}
+        for j, (i, o) in enumerate(owner):
+            w = float("inf") if ovf[j][0] else float(sum(int(x) for x in lvl[j][0][:cands[j].n_ops]))
+            best.setdefault(i, []).append((w, o))
+        out = []
+        for i in range(len(plans)):
+            h_work = best[i][0][0]
+            w, o = min(best[i], key=lambda t: t[0])
+            out.append((o, True) if o != hs[i] and w < (1.0 - margin) * h_work else (hs[i], False))
+        return out
 
     def choose(self, plan, x, margin=0.25):
         """(order, used_model): the predicted cheapest valid order, or the heuristic

@@ -5,10 +5,12 @@
 c1  -kc 3 on R-MAT scale 16, edge factor 16, seed 1, ids ascending with degree
     (the degree-ordered orientation), one view holding every source.
 c3  64 random connected patterns (3-6 vertices, p = 0.5, seed 3) x 16 Chung-Lu
-    views (exponent U[2.1, 2.8], edges log-uniform in [1e5, e_max], max degree
-    1e4, seed 3): the persistent batched launch against the plain level-wise
-    engine view after view, at identical counts.  Patterns whose sampled work
-    exceeds --max-work on some view are left out and listed.
+    views (exponent U[2.1, 2.8], edges log-uniform in [1e5, e_max] (default 1e6;
+    the configuration's 1e7 with --e-max 1e7), max degree 1e4, seed 3): the
+    persistent batched (hybrid) run and, with --learned, the batched run over the
+    learned planner's orders, against the plain level-wise engine with the
+    heuristic order view after view, at identical counts.  Patterns whose sampled
+    work exceeds --max-work on some view are left out and listed.
 c4  the learned planner on c3-distributed (pattern, view) pairs (seed 4): the
     network is trained by the library's MLP kernels on measured per-op work of
     candidate orders; held-out pairs report the work of the heuristic order and
@@ -69,6 +71,22 @@ def _screen(plans, views, stride, step_budget, device=0):
     return lvl.sum(axis=2) * stride, ovf
 
 
+def _train_planner(args):
+    """A planner trained on c4-distributed pairs (seed 4), or loaded from --model."""
+    model = lp.LearnedPlanner()
+    if args.model:
+        model.load(args.model)
+        return model, 0.0
+    views = [degree_relabel(g)[0] for g in wl.chung_lu_views(args.views, seed=4, e_min=2e4, e_max=2e5, max_degree=2000)]
+    pats = wl.random_patterns(args.patterns, seed=4)
+    sampler = lp.Sampler(views, roots_per_view=256, seed=1, step_budget=500_000)
+    pairs = [(pi, vi) for pi in range(len(pats)) for vi in range(len(views))]
+    t = time.perf_counter()
+    X, Y, M, _ = lp.make_examples(sampler, pats, pairs, orders_per_pair=8, seed=1)
+    model.train(X, Y, M, epochs=150)
+    return model, time.perf_counter() - t
+
+
 def run_c3(args):
     views = [degree_relabel(g)[0] for g in wl.chung_lu_views(16, seed=3, e_max=args.e_max)]
     pats = wl.random_patterns(64, seed=3)
@@ -76,7 +94,7 @@ def run_c3(args):
     keep = [i for i in range(len(pats)) if not ovf[i].any() and work[i].max() < args.max_work]
     plans = [pats[i] for i in keep]
     V = max(g.V for g in views)
-    # batched: every (pattern, view) pair in one persistent launch
+    # batched: every (pattern, view) pair in one persistent (hybrid) run
     with Engine(V, plans) as e:
         ids = [e.add_view(g) for g in views]
         e.set_profiling(True)
@@ -85,7 +103,39 @@ def run_c3(args):
         batched = e.run_batched(ids)
         b_wall = time.perf_counter() - t
         st = e.batch_stats()
-        b_ms, tasks = st.ms, st.tasks
+        b_ms, tasks, b_level = st.ms, st.tasks, st.level_pairs
+    learned = None
+    if args.learned:
+        # batched + learned: the planner picks one order per (pattern, view) (verified
+        # on a root sample of that view), then one hybrid run over the chosen plans
+        model, t_train = _train_planner(args)
+        sampler = lp.Sampler(views, roots_per_view=256, seed=1, step_budget=500_000)
+        t = time.perf_counter()
+        chosen = [model.choose_verified_many(plans, sampler, vi, k=4) for vi in range(len(views))]
+        t_plan = time.perf_counter() - t
+        model.close()
+        uniq, pair_list = [], []
+        for vi in range(len(views)):
+            for pi, (order, _) in enumerate(chosen[vi]):
+                key = (pi, tuple(order))
+                if key not in uniq:
+                    uniq.append(key)
+                pair_list.append((uniq.index(key), vi))
+        lplans = [lp.plan_reorder(plans[pi], o) for pi, o in uniq]
+        with Engine(V, lplans) as e:
+            ids = [e.add_view(g) for g in views]
+            e.set_profiling(True)
+            e.run_pairs([(a, ids[b]) for a, b in pair_list])  # warm-up
+            t = time.perf_counter()
+            got = e.run_pairs([(a, ids[b]) for a, b in pair_list])
+            l_wall = time.perf_counter() - t
+            lst = e.batch_stats()
+        lcounts = [[0] * len(views) for _ in plans]
+        for (a, vi), c in zip(pair_list, got):
+            lcounts[uniq[a][0]][vi] = c
+        learned = {"wall_ms": l_wall * 1e3, "device_ms": lst.ms, "level_pairs": int(lst.level_pairs), "tasks": int(lst.tasks),
+                   "orders_changed": sum(int(took) for row in chosen for _, took in row), "plan_s": t_plan, "train_s": t_train,
+                   "counts": lcounts}
     # plain: the level-wise engine, one view after the other (uploads outside the timing)
     plain = [[0] * len(views) for _ in plans]
     p_ms = p_wall = 0.0
@@ -106,11 +156,17 @@ def run_c3(args):
                 p_ms += sum(s.op_ms[j] for j in range(p.n_ops))
                 launches += sum(s.op_launches[j] for j in range(p.n_ops))
     total = sum(sum(r) for r in plain)
-    return {"config": "c3", "views": [(g.V, g.E) for g in views], "patterns_run": len(keep), "patterns_left_out": [i for i in range(len(pats)) if i not in keep],
-            "identical_counts": [list(map(int, r)) for r in batched] == plain, "matches": int(total),
-            "batched": {"device_ms": b_ms, "wall_ms": b_wall * 1e3, "launches": 1, "tasks": int(tasks)},
-            "plain": {"device_ms": p_ms, "wall_ms": p_wall * 1e3, "launches": int(launches)},
-            "speedup_wall": p_wall / b_wall if b_wall else None}
+    out = {"config": "c3", "views": [(g.V, g.E) for g in views], "patterns_run": len(keep),
+           "patterns_left_out": [i for i in range(len(pats)) if i not in keep],
+           "identical_counts": [list(map(int, r)) for r in batched] == plain, "matches": int(total),
+           "batched": {"device_ms": b_ms, "wall_ms": b_wall * 1e3, "tasks": int(tasks), "level_pairs": int(b_level)},
+           "plain": {"device_ms": p_ms, "wall_ms": p_wall * 1e3, "launches": int(launches)},
+           "speedup_wall": p_wall / b_wall if b_wall else None}
+    if learned:
+        out["learned_identical_counts"] = learned.pop("counts") == plain
+        out["batched_learned"] = learned
+        out["speedup_learned_wall"] = p_wall / (learned["wall_ms"] / 1e3) if learned["wall_ms"] else None
+    return out
 
 
 def run_c4(args):
@@ -139,6 +195,8 @@ def run_c4(args):
         cnt, lvl, ovf = check.evaluate(plans, vi)
         heur += sum(int(x) for x in lvl[0][0][:plans[0].n_ops])
         learned += sum(int(x) for x in lvl[1][0][:plans[1].n_ops])
+    if args.save:
+        model.save(args.save)
     model.close()
     return {"config": "c4", "train_pairs": cut, "held_out_pairs": len(pairs) - cut, "examples": int(len(X)), "log_s": t_logs, "train_s": t_train,
             "loss_first": losses[0], "loss_last": losses[-1], "model_order_used": used,
@@ -176,9 +234,12 @@ def main(argv=None):
     ap.add_argument("--views", type=int, default=8)
     ap.add_argument("--patterns", type=int, default=96)
     ap.add_argument("--scale-down", type=int, default=1)
+    ap.add_argument("--learned", action="store_true", help="c3: also run batched + learned orders")
+    ap.add_argument("--model", default=None, help="c3 --learned: planner parameters (.npy from c4 --save)")
+    ap.add_argument("--save", default=None, help="c4: write the trained planner's parameters here")
     args = ap.parse_args(argv)
     if args.e_max is None:
-        args.e_max = {"c3": 1e7, "c4": 2e5}.get(args.config, 1e7)
+        args.e_max = {"c3": 1e6, "c4": 2e5}.get(args.config, 1e7)
     out = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
     print(json.dumps(out), flush=True)
     return 0
