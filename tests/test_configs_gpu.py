@@ -48,7 +48,7 @@ def test_c2_whole_graph_and_bins(vs, rmat22):
 def test_c2_root_sample_against_oracle(vs, orc, rmat22):
     g, plans = rmat22
     rng = np.random.default_rng(21)
-    src = np.sort(rng.choice(g.V, size=3000, replace=False)).astype(np.uint32)
+    src = np.sort(rng.choice(g.V, size=600, replace=False)).astype(np.uint32)
     with vs.Engine(g.V, plans) as e:
         e.set_option("c4_aggregate", 0)  # per-root attribution of the plan
         e.transfer_view(g, src)

@@ -529,7 +529,13 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
 // Same result as expanding the children and running COMPUTE_COUNT on them
 // (src/executor/ops/materialize.h, src/executor/ops/compute_count.h).
 // ---------------------------------------------------------------------------
-constexpr int kStageCap = 1536;  // u32 per warp (8 warps: 48 KB of static shared memory per block)
+constexpr int kStageCap = 1408;   // u32 per warp
+constexpr int kFilterWords = 128;  // 4096-bit membership filter of the stage per warp
+// 8 warps x (1408 + 128) u32 = 48 KB of static shared memory per block
+static_assert(8 * (kStageCap + kFilterWords) * 4 <= 48 * 1024, "static shared memory");
+
+// bit of x in the stage's filter (multiplicative hash, top 12 bits)
+__device__ __forceinline__ uint32_t filter_bit(uint32_t x) { return (x * 2654435761u) >> 20; }
 constexpr uint32_t kLaneSlice = 16;
 
 struct FusedDesc {
@@ -579,9 +585,11 @@ template <int NK, bool kOther>
 __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
                                                    unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
   __shared__ uint32_t stage[8][kStageCap];
+  __shared__ uint32_t filt[8][kFilterWords];
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
   const unsigned lane = lane_id();
   uint32_t* I = stage[threadIdx.x / kWarp];
+  uint32_t* F = filt[threadIdx.x / kWarp];
   const OpDesc& d = fd.known;
   const uint32_t excl_child = (fd.has_cond_u && fd.cond_u_op == VSGM_NON_EQUAL) ? 1u : 0u;
   unsigned long long acc = 0, acc_bytes = 0;
@@ -630,6 +638,16 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
       __syncwarp();
       if (lane == 0) acc_bytes += 4ull * (L.pe - L.ps) + 16ull * NK + 4ull * d.nm;
       if (ni == 0) continue;
+      // membership filter of I: a walk over N(c) skips the stage search for values
+      // whose bit is clear (most of them)
+#pragma unroll
+      for (int q = 0; q < kFilterWords / kWarp; q++) F[q * kWarp + lane] = 0u;
+      __syncwarp();
+      for (uint32_t j = lane; j < ni; j += kWarp) {
+        const uint32_t b = filter_bit(I[j]);
+        atomicOr(F + (b >> 5), 1u << (b & 31));
+      }
+      __syncwarp();
       for (uint32_t k0 = 0; k0 < nc; k0 += kWarp) {
         // pass 1, one child per lane; long slices are left for pass 2
         const uint32_t k = k0 + lane;
@@ -681,6 +699,8 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
             uint32_t cur = ia;
             for (uint64_t j = s2 + lane; j < e2; j += kWarp) {
               const uint32_t x = __ldg(ci + j);
+              const uint32_t b = filter_bit(x);
+              if (!((F[b >> 5] >> (b & 31)) & 1u)) continue;  // certainly not in I
               const uint32_t r = smem_lower_bound(I, cur, ib, x);
               cur = r;
               if (r < ib && I[r] == x && x != excl) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
@@ -805,37 +825,6 @@ __global__ void k_expand(Frame in, Expand x, const uint64_t* __restrict__ off, u
 }
 
 // ---------------------------------------------------------------------------
-// Load-balanced walk over up to 32 short rows at once: lane l owns the range
-// [a_l, a_l + n_l) of ci (n_l = 0 for no row); every round the 32 lanes read 32
-// consecutive entries of the concatenated ranges (owner found by a 5-step search
-// over the inclusive prefix of n), so the loads of a warp are independent instead
-// of one row's chain at a time.  f(owner's tag, entry value) is called per entry.
-// ---------------------------------------------------------------------------
-template <typename F>
-__device__ __forceinline__ void warp_rows(uint64_t a, uint64_t n, uint32_t tag, const uint32_t* __restrict__ ci, F&& f) {
-  const unsigned lane = lane_id();
-  uint64_t inc = n;
-#pragma unroll
-  for (int o = 1; o < kWarp; o <<= 1) {
-    const uint64_t t = __shfl_up_sync(kFull, inc, o);
-    if (lane >= (unsigned)o) inc += t;
-  }
-  const uint64_t total = __shfl_sync(kFull, inc, kWarp - 1);
-  const uint64_t excl = inc - n;
-  for (uint64_t base = 0; base < total; base += kWarp) {
-    const uint64_t t = base + lane;
-    unsigned lo = 0;  // lanes whose inclusive prefix is <= t (the prefix is non-decreasing)
-#pragma unroll
-    for (unsigned step = 16; step > 0; step >>= 1)
-      if (__shfl_sync(kFull, inc, lo + step - 1) <= t) lo += step;
-    const unsigned owner = lo < kWarp ? lo : kWarp - 1;
-    const uint64_t oa = __shfl_sync(kFull, a, owner), oe = __shfl_sync(kFull, excl, owner);
-    const uint32_t otag = __shfl_sync(kFull, tag, owner);
-    if (t < total) f(otag, __ldg(ci + oa + (t - oe)));
-  }
-}
-
-// ---------------------------------------------------------------------------
 // 4-cycle count by wedge aggregation.  Every 4-cycle is counted once, at its
 // largest vertex u: for each neighbour v < u and each w in N(v) with w < u,
 // L[w] counts the wedges u-v-w; the cycles closed at u are sum C(L[w], 2)
@@ -864,21 +853,17 @@ __global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict
     const unsigned long long r = s_root;
     if (r >= n_roots) break;
     const uint32_t u = __ldg(roots + r);
-    const uint64_t ua = __ldg(rp + u);
-    const uint64_t ub = lower_bound(ci, ua, __ldg(rp + u + 1), u);  // centres v < u
-    // wedges: each warp takes 32 centres at a time, one per lane, and walks their
-    // rows below u together
-    for (uint64_t k0 = ua + (uint64_t)warp * kWarp; k0 < ub; k0 += (uint64_t)nwarps * kWarp) {
-      const uint64_t k = k0 + lane;
-      uint64_t va = 0, vn = 0;
-      if (k < ub) {
-        const uint32_t v = __ldg(ci + k);
-        va = __ldg(rp + v);
-        vn = lower_bound(ci, va, __ldg(rp + v + 1), u) - va;
-      }
-      warp_rows(va, vn, 0u, ci, [&](uint32_t, uint32_t w) {
+    const uint64_t ua = __ldg(rp + u), uz = __ldg(rp + u + 1);
+    // wedges: warp per neighbour v < u, lanes over N(v) below u
+    for (uint64_t k = ua + warp; k < uz; k += nwarps) {
+      const uint32_t v = __ldg(ci + k);
+      if (v >= u) break;  // rows are sorted
+      const uint64_t va = __ldg(rp + v), vz = __ldg(rp + v + 1);
+      for (uint64_t j = va + lane; j < vz; j += kWarp) {
+        const uint32_t w = __ldg(ci + j);
+        if (w >= u) break;
         if (atomicAdd(L + w, 1u) == 0u) touched[atomicAdd(&s_touched, 1u)] = w;
-      });
+      }
     }
     __syncthreads();
     const unsigned n = s_touched;
@@ -951,20 +936,19 @@ __global__ void __launch_bounds__(256) k_c4_group_wedges(const uint64_t* __restr
   const uint64_t total = G.vbeg[G.n];
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
   const unsigned lane = lane_id();
-  // each warp takes 32 centres at a time (one per lane, possibly of different
-  // roots of the group) and walks their rows below their roots together
-  for (uint64_t i0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp * kWarp; i0 < total; i0 += warps * kWarp) {
-    const uint64_t i = i0 + lane;
-    uint64_t va = 0, vn = 0;
+  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < total; i += warps) {
     uint32_t g = 0;
-    if (i < total) {
-      while (g + 1 < G.n && i >= G.vbeg[g + 1]) g++;
-      const uint32_t u = G.root[g];
-      const uint32_t v = __ldg(ci + __ldg(rp + u) + (i - G.vbeg[g]));  // v < u: the row is sorted
-      va = __ldg(rp + v);
-      vn = lower_bound(ci, va, __ldg(rp + v + 1), u) - va;
+    while (g + 1 < G.n && i >= G.vbeg[g + 1]) g++;
+    const uint32_t u = G.root[g];
+    const uint32_t v = __ldg(ci + __ldg(rp + u) + (i - G.vbeg[g]));  // v < u: the row is sorted
+    uint32_t* Lg = L + (uint64_t)g * stride;
+    const uint64_t z = __ldg(rp + v + 1);
+    for (uint64_t base = __ldg(rp + v); base < z; base += kWarp) {
+      const uint64_t j = base + lane;
+      const uint32_t w = j < z ? __ldg(ci + j) : u;
+      if (w < u) atomicAdd(Lg + w, 1u);
+      if (__any_sync(kFull, w >= u)) break;
     }
-    warp_rows(va, vn, g, ci, [&](uint32_t og, uint32_t w) { atomicAdd(L + (uint64_t)og * stride + w, 1u); });
   }
 }
 
