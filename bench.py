@@ -18,7 +18,9 @@ e2e     = the same through the C ABI from pinned host buffers: view upload +
           match + count read-back inside the timed region
 roofline: dominant kernel (COMPUTE_COUNT) algorithmic bytes / its device time
 cpu_baseline / --impl reference: the CPU restatement of the reference executor
-          (oracle/) on a time-boxed random sample of roots, all host cores.
+          (oracle/) on a time-boxed random sample of roots, all host cores;
+          cpu_baseline.view_stages: the reference's own .bin reader and view
+          materialisation (compiled from its sources) beside ours, on host and device.
 """
 import argparse
 import json
@@ -144,6 +146,41 @@ def cpu_sample_rate(g, plans, seconds, threads):
     return total_count / total_time, total_count, total_time, roots_done
 
 
+def view_stage_times(vs, eng, g, threads):
+    """The view-producing stages beside the match: the reference's own .bin reader
+    and ViewBin::Materialize (compiled from its sources into oracle/_ref, when that
+    build exists), against this library's bulk reader, host halo build and device
+    halo build, on the workload graph as one 2-hop view bin.  Milliseconds."""
+    import tempfile
+    out = {"view": "1 bin holding every source, hop 2"}
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "g.bin")
+        vs.write_csr_bin(path, g)
+        vs.write_vbmap(path + ".2.hop.vbmap", np.zeros(g.V, np.int32), 1)
+        t = time.perf_counter()
+        h = vs.read_csr_bin(path)
+        out["read_bin_ms"] = (time.perf_counter() - t) * 1e3
+        src = np.arange(g.V, dtype=np.uint32)
+        t = time.perf_counter()
+        vs.materialize_view(h, src, 2, 0, threads)
+        out["materialize_host_ms"] = (time.perf_counter() - t) * 1e3
+        import torch
+        eng.upload_graph(h)
+        eng.materialize_view(src, 2)  # warm-up
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        eng.materialize_view(src, 2)
+        out["materialize_device_ms"] = (time.perf_counter() - t) * 1e3
+        stages = os.path.join(ROOT, "oracle", "_ref", "ref_cpu_stages")
+        if os.path.exists(stages):
+            r = subprocess.run([stages, "read", path], capture_output=True, text=True, timeout=600)
+            out["reference_read_bin_ms"] = float(r.stdout.strip().splitlines()[-1].split()[-1])
+            r = subprocess.run([stages, "views", path, path + ".2.hop.vbmap", "2", "0", str(threads)], capture_output=True, text=True, timeout=600)
+            out["reference_materialize_ms"] = float(r.stdout.strip().splitlines()[-1].split()[-1])
+            out["reference"] = "GraphIO::ReadCSRBinFile, ViewBin::Materialize compiled from the reference sources"
+    return out
+
+
 def run_reference(args):
     import torch.distributed as dist  # noqa: F401  (rank handling only)
     rank = int(os.environ.get("RANK", "0"))
@@ -185,6 +222,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--queries", default="kc4,p1,p2", help="comma list of kcK / pN (default: the workload's three)")
     ap.add_argument("--option", action="append", default=[], help="engine knob name=value (vsgm_set_option), repeatable")
+    ap.add_argument("--no-stages", action="store_true", help="skip the view-stage timings of the CPU leg")
     ap.add_argument("--hbm-gb", type=float, default=0.0,
                     help="engine working budget in GB (0: 90%% of free HBM); profiler captures use a few GB")
     args = ap.parse_args()
@@ -305,6 +343,11 @@ def main():
         rate, cnt, secs, nroots = cpu_sample_rate(g, plans, args.cpu_seconds, threads)
         cpu = {"value": rate, "unit": "matches/s", "cores": threads, "kind": "port",
                "sample": f"{nroots} random roots (time-boxed {args.cpu_seconds}s over the {len(plans)} queries), matches/s = sampled matches / seconds"}
+        if not args.no_stages:
+            try:
+                cpu["view_stages"] = view_stage_times(vs, eng, g, threads)
+            except Exception as ex:  # the stages are a side measurement; the line still prints
+                cpu["view_stages"] = {"error": str(ex)}
 
     if rank == 0:
         out = {"metric": "matches/s", "value": value, "unit": "matches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
