@@ -233,6 +233,8 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   staged set walks its own adjacency range coalesced (probing the stage) unless
  *   that range is this many times longer than the slice, then it gallops (0: always
  *   gallop);
+ *   "lane_slice" (default 16): in the fused tail a child whose slice of the staged
+ *   set is at most this long is handled by one lane, longer ones by the whole warp;
  *   "c4_heavy" (default 2^20): roots with at least this many wedges are counted by
  *   groups sharing the whole GPU with L2-resident counters (0: every root);
  *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT

@@ -293,10 +293,13 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
                 e.match()
                 assert e.counts() == want, (ratio, lane)
         for walk in (0, 1, 8, 1000):
-            e.set_option("walk_ratio", walk)
-            e.reset_counts()
-            e.match()
-            assert e.counts() == want, walk
+            for ls in (0, 16, 4096):
+                e.set_option("walk_ratio", walk)
+                e.set_option("lane_slice", ls)
+                e.reset_counts()
+                e.match()
+                assert e.counts() == want, (walk, ls)
+        e.set_option("lane_slice", 16)
         report = autotune(e, len(plans), stride=4)
         assert [r["plan"] for r in report] == list(range(len(plans)))
         e.match()

@@ -122,6 +122,7 @@ struct vsgm_engine {
     bool set_reuse = true;           // COMPUTE o + COMPUTE_COUNT w over the same set: count pairs of one intersection
     uint64_t c4_heavy = 1ull << 20;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
     uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
+    uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -589,6 +590,7 @@ struct vsgm_engine {
     fd.u = (uint8_t)u;
     fd.stage_cap = cur.stage_cap;
     fd.walk_ratio = cur.walk_ratio;
+    fd.lane_slice = cur.lane_slice;
     fd.up = (fd.has_cond_u && fd.cond_u_op == VSGM_LARGER_THAN) ? upper_offsets() : nullptr;
     fd.other = -1;
     const vsgm_vgroup& cu = p.computed_unmat[i + 1];
@@ -1370,6 +1372,11 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   }
   if (n == "c4_aggregate") {
     for (int k = lo; k < hi; k++) e->knobs[k].c4_aggregate = value != 0;
+    return VSGM_OK;
+  }
+  if (n == "lane_slice") {
+    if (value < 0 || value > 4096) return engine_fail(e, VSGM_EINVAL, "lane_slice must be 0..4096");
+    for (int k = lo; k < hi; k++) e->knobs[k].lane_slice = (uint32_t)value;
     return VSGM_OK;
   }
   if (n == "walk_ratio") {

@@ -536,7 +536,7 @@ static_assert(8 * (kStageCap + kFilterWords) * 4 <= 48 * 1024, "static shared me
 
 // bit of x in the stage's filter (multiplicative hash, top 12 bits)
 __device__ __forceinline__ uint32_t filter_bit(uint32_t x) { return (x * 2654435761u) >> 20; }
-constexpr uint32_t kLaneSlice = 16;
+constexpr uint32_t kLaneSlice = 16;  // default: children with longer slices go to the whole-warp pass
 
 struct FusedDesc {
   OpDesc known;        // w's backward lists and conditions that do not involve u (slots into the parent gather)
@@ -547,6 +547,7 @@ struct FusedDesc {
   uint8_t other_op;
   uint32_t stage_cap;  // <= kStageCap; smaller values force the per-child path
   uint32_t walk_ratio; // a heavy child walks N(c) (probing the stage) unless N(c)'s part is this many times longer
+  uint32_t lane_slice; // children whose slice is longer go to the whole-warp pass
   const uint32_t* up;  // per vertex c: offset of the first neighbour > c in N(c) (cond_u_op LARGER_THAN), else null
 };
 
@@ -656,7 +657,7 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
           const uint32_t c = __ldg(cs + k);
           uint32_t ia, ib;
           child_slice(fd, w, I, ni, c, &ia, &ib);
-          if (ib - ia > kLaneSlice) {
+          if (ib - ia > fd.lane_slice) {
             heavy = true;
           } else if (ia < ib) {
             const uint64_t a0 = __ldg(rp + c), z0 = __ldg(rp + c + 1);
