@@ -235,14 +235,14 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   gallop);
  *   "lane_slice" (default 16): in the fused tail a child whose slice of the staged
  *   set is at most this long is handled by one lane, longer ones by the whole warp;
- *   "c4_heavy" (default 2^20): roots with at least this many wedges are counted by
+ *   "c4_heavy" (default 2^18): roots with at least this many wedges are counted by
  *   groups sharing the whole GPU with L2-resident counters (0: every root);
  *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT
  *   of a vertex with the same backward lists and conditions (the diamond's tail)
  *   counts the pairs of one intersection instead of intersecting twice;
  *   "lane_merge" (default 0): counting kernels merge two such lists with each lane
  *   walking its own chunk instead of 32-element warp windows;
- *   "hybrid_steps" (engine-wide, default 2^17): vsgm_run_batched runs every pair in
+ *   "hybrid_steps" (engine-wide, default 2^14): vsgm_run_batched runs every pair in
  *   the persistent launch with this per-task step bound and counts the pairs it
  *   stopped again with the level-wise engine on their resident view (0: the
  *   persistent launch alone, unbounded);

@@ -48,13 +48,16 @@ def test_c2_whole_graph_and_bins(vs, rmat22):
 def test_c2_root_sample_against_oracle(vs, orc, rmat22):
     g, plans = rmat22
     rng = np.random.default_rng(21)
-    src = np.sort(rng.choice(g.V, size=600, replace=False)).astype(np.uint32)
-    with vs.Engine(g.V, plans) as e:
-        e.set_option("c4_aggregate", 0)  # per-root attribution of the plan
-        e.transfer_view(g, src)
-        e.match()
-        got = e.counts()
-    assert got == [orc.count(p, g, src) for p in plans]
+    # the 4-cycle plan walks hub lists from every root: a smaller sample keeps the
+    # oracle within seconds
+    for sample, chosen in ((600, [plans[0], plans[2]]), (120, [plans[1]])):
+        src = np.sort(rng.choice(g.V, size=sample, replace=False)).astype(np.uint32)
+        with vs.Engine(g.V, chosen) as e:
+            e.set_option("c4_aggregate", 0)  # per-root attribution of the plan
+            e.transfer_view(g, src)
+            e.match()
+            got = e.counts()
+        assert got == [orc.count(p, g, src) for p in chosen]
 
 
 @pytest.mark.skipif(os.environ.get("VSGM_LARGE") != "1", reason="65M-vertex graph: set VSGM_LARGE=1")

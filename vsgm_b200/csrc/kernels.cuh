@@ -640,15 +640,19 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
       if (lane == 0) acc_bytes += 4ull * (L.pe - L.ps) + 16ull * NK + 4ull * d.nm;
       if (ni == 0) continue;
       // membership filter of I: a walk over N(c) skips the stage search for values
-      // whose bit is clear (most of them)
+      // whose bit is clear (most of them).  Only a stage longer than lane_slice can
+      // have a heavy child, so smaller stages skip building it.
+      const bool filtered = ni > fd.lane_slice;
+      if (filtered) {
 #pragma unroll
-      for (int q = 0; q < kFilterWords / kWarp; q++) F[q * kWarp + lane] = 0u;
-      __syncwarp();
-      for (uint32_t j = lane; j < ni; j += kWarp) {
-        const uint32_t b = filter_bit(I[j]);
-        atomicOr(F + (b >> 5), 1u << (b & 31));
+        for (int q = 0; q < kFilterWords / kWarp; q++) F[q * kWarp + lane] = 0u;
+        __syncwarp();
+        for (uint32_t j = lane; j < ni; j += kWarp) {
+          const uint32_t b = filter_bit(I[j]);
+          atomicOr(F + (b >> 5), 1u << (b & 31));
+        }
+        __syncwarp();
       }
-      __syncwarp();
       for (uint32_t k0 = 0; k0 < nc; k0 += kWarp) {
         // pass 1, one child per lane; long slices are left for pass 2
         const uint32_t k = k0 + lane;
@@ -701,7 +705,7 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
             for (uint64_t j = s2 + lane; j < e2; j += kWarp) {
               const uint32_t x = __ldg(ci + j);
               const uint32_t b = filter_bit(x);
-              if (!((F[b >> 5] >> (b & 31)) & 1u)) continue;  // certainly not in I
+              if (filtered && !((F[b >> 5] >> (b & 31)) & 1u)) continue;  // certainly not in I
               const uint32_t r = smem_lower_bound(I, cur, ib, x);
               cur = r;
               if (r < ib && I[r] == x && x != excl) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;

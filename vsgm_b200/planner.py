@@ -264,6 +264,42 @@ class LearnedPlanner:
             out.append((o, True) if o != hs[i] and w < (1.0 - margin) * h_work else (hs[i], False))
         return out
 
+    def choose_timed_many(self, plans, sampler, view_index, k=4, stride=16, margin=0.1):
+        """Like choose_verified_many, but the proposals are judged by time: the
+        level-wise engine (the one the heavy pairs run on) times the heuristic order
+        and the network's k proposals of every pattern on every stride-th root of the
+        view, and the fastest replaces the heuristic order if it saves at least
+        `margin` of its time.  Partial-match counts ignore how long the intersected
+        lists are; time does not."""
+        g = sampler.views[view_index]
+        hs = [heuristic_order(p) for p in plans]
+        _, lvl0, _ = sampler.evaluate(list(plans), view_index)
+        X = np.stack([features(p, sampler.hist[view_index], lvl0[i][0]) for i, p in enumerate(plans)])
+        pred = self.predict(X)
+        cands, owner = [], []
+        for i, p in enumerate(plans):
+            ranked = sorted((o for o in valid_orders(p) if o != hs[i]), key=lambda o: pred[i][order_index(o)])
+            for o in [hs[i]] + ranked[:k]:
+                cands.append(plan_reorder(p, o))
+                owner.append((i, o))
+        with Engine(g.V, cands, device=sampler.device) as e:
+            e.transfer_view(g, np.arange(0, g.V, stride, dtype=np.uint32))
+            e.set_profiling(True)
+            e.match()
+            ms = []
+            for j, c in enumerate(cands):
+                st = e.stats(j)
+                ms.append(sum(st.op_ms[t] for t in range(c.n_ops)))
+        best = {}
+        for j, (i, o) in enumerate(owner):
+            best.setdefault(i, []).append((ms[j], o))
+        out = []
+        for i in range(len(plans)):
+            h_ms = best[i][0][0]
+            t, o = min(best[i], key=lambda x: x[0])
+            out.append((o, True) if o != hs[i] and t < (1.0 - margin) * h_ms else (hs[i], False))
+        return out
+
     def choose(self, plan, x, margin=0.25):
         """(order, used_model): the predicted cheapest valid order, or the heuristic
         one when it is not predicted to be cheaper by at least `margin` (log units)."""

@@ -106,12 +106,13 @@ def run_c3(args):
         b_ms, tasks, b_level = st.ms, st.tasks, st.level_pairs
     learned = None
     if args.learned:
-        # batched + learned: the planner picks one order per (pattern, view) (verified
-        # on a root sample of that view), then one hybrid run over the chosen plans
+        # batched + learned: the planner proposes orders per (pattern, view), the
+        # level-wise engine times them on a root sample of that view, then one
+        # hybrid run over the chosen plans
         model, t_train = _train_planner(args)
         sampler = lp.Sampler(views, roots_per_view=256, seed=1, step_budget=500_000)
         t = time.perf_counter()
-        chosen = [model.choose_verified_many(plans, sampler, vi, k=4) for vi in range(len(views))]
+        chosen = [model.choose_timed_many(plans, sampler, vi, k=4) for vi in range(len(views))]
         t_plan = time.perf_counter() - t
         model.close()
         uniq, pair_list = [], []
