@@ -220,7 +220,7 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   "fuse_tail" (default 1): a MATERIALIZE followed by the final COMPUTE_COUNT runs as
  *   one kernel that stages the parent's shared lists in shared memory instead of
  *   expanding the children;
- *   "stage_cap" (default and maximum 1408): largest shared list staged per warp, in
+ *   "stage_cap" (default and maximum 1536): largest shared list staged per warp, in
  *   vertex ids; larger ones take the per-child intersection;
  *   "merge_ratio" (default 4): two lists whose restricted lengths are within this
  *   ratio are intersected by a coalesced merge, otherwise by galloping (0: always

@@ -211,11 +211,11 @@ def _hub_graph(vs, leaves=2000, chords=3000, seed=4):
 def test_fused_tail_large_staged_sets(vs, orc, graphs):
     """Shared lists larger than the stage take the per-child path (natural hub, and forced)."""
     hub, _ = vs.degree_relabel(_hub_graph(vs))
-    assert hub.degrees().max() > 1408
+    assert hub.degrees().max() > 1536
     plans = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(8)]
     for g in (hub, graphs["rmat8"]):
         want = [orc.count(p, g) for p in plans]
-        for cap in (1408, 16, 0):
+        for cap in (1536, 16, 0):
             with vs.Engine(g.V, plans) as e:
                 e.set_option("stage_cap", cap)
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))

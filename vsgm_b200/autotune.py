@@ -14,7 +14,7 @@ CANDIDATES = {
     "fuse_tail": (1, 0),
     "merge_ratio": (0, 4, 16),
     "lane_merge": (0, 1),
-    "stage_cap": (1408, 384),
+    "stage_cap": (1536, 384),
     "walk_ratio": (8, 1),
 }
 

@@ -529,13 +529,7 @@ __global__ void __launch_bounds__(256) k_compute_count(Frame f, OpDesc d, const 
 // Same result as expanding the children and running COMPUTE_COUNT on them
 // (src/executor/ops/materialize.h, src/executor/ops/compute_count.h).
 // ---------------------------------------------------------------------------
-constexpr int kStageCap = 1408;   // u32 per warp
-constexpr int kFilterWords = 128;  // 4096-bit membership filter of the stage per warp
-// 8 warps x (1408 + 128) u32 = 48 KB of static shared memory per block
-static_assert(8 * (kStageCap + kFilterWords) * 4 <= 48 * 1024, "static shared memory");
-
-// bit of x in the stage's filter (multiplicative hash, top 12 bits)
-__device__ __forceinline__ uint32_t filter_bit(uint32_t x) { return (x * 2654435761u) >> 20; }
+constexpr int kStageCap = 1536;  // u32 per warp (8 warps: 48 KB of static shared memory per block)
 constexpr uint32_t kLaneSlice = 16;  // default: children with longer slices go to the whole-warp pass
 
 struct FusedDesc {
@@ -586,11 +580,9 @@ template <int NK, bool kOther>
 __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
                                                    unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
   __shared__ uint32_t stage[8][kStageCap];
-  __shared__ uint32_t filt[8][kFilterWords];
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
   const unsigned lane = lane_id();
   uint32_t* I = stage[threadIdx.x / kWarp];
-  uint32_t* F = filt[threadIdx.x / kWarp];
   const OpDesc& d = fd.known;
   const uint32_t excl_child = (fd.has_cond_u && fd.cond_u_op == VSGM_NON_EQUAL) ? 1u : 0u;
   unsigned long long acc = 0, acc_bytes = 0;
@@ -639,20 +631,6 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
       __syncwarp();
       if (lane == 0) acc_bytes += 4ull * (L.pe - L.ps) + 16ull * NK + 4ull * d.nm;
       if (ni == 0) continue;
-      // membership filter of I: a walk over N(c) skips the stage search for values
-      // whose bit is clear (most of them).  Only a stage longer than lane_slice can
-      // have a heavy child, so smaller stages skip building it.
-      const bool filtered = ni > fd.lane_slice;
-      if (filtered) {
-#pragma unroll
-        for (int q = 0; q < kFilterWords / kWarp; q++) F[q * kWarp + lane] = 0u;
-        __syncwarp();
-        for (uint32_t j = lane; j < ni; j += kWarp) {
-          const uint32_t b = filter_bit(I[j]);
-          atomicOr(F + (b >> 5), 1u << (b & 31));
-        }
-        __syncwarp();
-      }
       for (uint32_t k0 = 0; k0 < nc; k0 += kWarp) {
         // pass 1, one child per lane; long slices are left for pass 2
         const uint32_t k = k0 + lane;
@@ -704,8 +682,6 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
             uint32_t cur = ia;
             for (uint64_t j = s2 + lane; j < e2; j += kWarp) {
               const uint32_t x = __ldg(ci + j);
-              const uint32_t b = filter_bit(x);
-              if (filtered && !((F[b >> 5] >> (b & 31)) & 1u)) continue;  // certainly not in I
               const uint32_t r = smem_lower_bound(I, cur, ib, x);
               cur = r;
               if (r < ib && I[r] == x && x != excl) acc += kOther ? count_vs(oset, on, &ocur, x, fd.other_op) : 1ull;
