@@ -63,9 +63,18 @@ uint64_t vsgm_plan_automorphisms(const vsgm_plan* p);
 /* Release memory this library allocated for the caller. */
 void vsgm_free(void* p);
 
-/* GraphIO::ReadCSRBinFile (src/graph/graph_io.h:57-100), as one bulk read.
- * *row_ptrs (V+1 entries) and *cols (E entries) are allocated here: vsgm_free. */
+/* GraphIO::ReadCSRBinFile (src/graph/graph_io.h:57-100), as parallel bulk reads
+ * (the reference reads one element per fread).  The file size must match its
+ * header exactly.  *row_ptrs (V+1 entries) and *cols (E entries) are allocated
+ * here: vsgm_free. */
 int vsgm_read_csr_bin(const char* path, uint64_t* V, uint64_t* E, uint64_t** row_ptrs, uint32_t** cols);
+
+/* The same reader in two steps, for callers that own the buffers (pinned host
+ * memory, for instance): the header (sizes checked against the file), then the
+ * arrays straight into row_ptrs[V+1] and cols[E] with `threads` parallel reads
+ * (0 = all cores). */
+int vsgm_csr_bin_header(const char* path, uint64_t* V, uint64_t* E);
+int vsgm_read_csr_bin_into(const char* path, uint64_t V, uint64_t E, uint64_t* row_ptrs, uint32_t* cols, int threads);
 
 /* GraphIO::WriteCSRBinFile (src/graph/graph_io.h:313-339). */
 int vsgm_write_csr_bin(const char* path, uint64_t V, uint64_t E, const uint64_t* row_ptrs, const uint32_t* cols);

@@ -58,6 +58,49 @@ def test_csr_bin_rejects_truncated_file(vs, tmp_path):
         vs.read_csr_bin(tmp_path / "missing.bin")
 
 
+def test_csr_bin_size_must_match_header(vs, tmp_path):
+    """Like the reference reader, the file must end right after the cols; the
+    allocating reader, the two-step reader and the driver's path agree."""
+    from vsgm_b200 import capi
+    g = vs.gen_rmat(7, 4, seed=3)
+    p = tmp_path / "g.bin"
+    vs.write_csr_bin(p, g)
+    good = p.read_bytes()
+    p.write_bytes(good + b"\0")  # one byte too many
+    with pytest.raises(vs.VsgmError):
+        vs.read_csr_bin(p)
+    bad = bytearray(good)
+    bad[16:24] = np.uint64(g.V + 1).tobytes()  # V that does not fit the size
+    p.write_bytes(bytes(bad))
+    with pytest.raises(vs.VsgmError):
+        vs.read_csr_bin(p)
+    p.write_bytes(good)
+    L = capi.lib()
+    import ctypes as C
+    rp = np.empty(g.V + 1, np.uint64)
+    ci = np.empty(g.E, np.uint32)
+    # the caller's sizes must be the file's
+    assert L.vsgm_read_csr_bin_into(str(p).encode(), g.V, g.E - 1, capi.ptr(rp, C.c_uint64), capi.ptr(ci, C.c_uint32), 2) != 0
+    V, E = C.c_uint64(), C.c_uint64()
+    rpp, cip = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+    assert L.vsgm_read_csr_bin(str(p).encode(), C.byref(V), C.byref(E), C.byref(rpp), C.byref(cip)) == 0
+    assert (V.value, E.value) == (g.V, g.E)
+    assert np.array_equal(np.ctypeslib.as_array(cip, shape=(g.E,)), g.cols)
+    L.vsgm_free(C.cast(rpp, C.c_void_p))
+    L.vsgm_free(C.cast(cip, C.c_void_p))
+
+
+def test_csr_bin_multi_chunk_parallel_read(vs, tmp_path):
+    """A file larger than one read chunk (64 MB), read with several threads."""
+    g = vs.gen_rmat(20, 16, seed=4)
+    assert 4 * g.E > (64 << 20)
+    p = tmp_path / "big.bin"
+    vs.write_csr_bin(p, g)
+    for threads in (1, 3, 0):
+        h = vs.read_csr_bin(p, threads=threads)
+        assert np.array_equal(h.row_ptrs, g.row_ptrs) and np.array_equal(h.cols, g.cols)
+
+
 def test_vbmap_round_trip(vs, tmp_path):
     bins = np.array([0, 2, 1, 1, 0, 2, 2], np.int32)
     p = tmp_path / "g.bin.2.hop.vbmap"

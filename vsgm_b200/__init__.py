@@ -128,11 +128,14 @@ def random_pattern(seed, counter, n_min=3, n_max=6, p=0.5):
     return n.value, [bits[i] for i in range(capi.MAX_QV)], ctr.value
 
 
-def read_csr_bin(path):
+def read_csr_bin(path, threads=0):
+    """The .bin file straight into numpy arrays (parallel bulk reads, no copy)."""
     V, E = C.c_uint64(), C.c_uint64()
-    rp, ci = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
-    capi.check(_L().vsgm_read_csr_bin(str(path).encode(), C.byref(V), C.byref(E), C.byref(rp), C.byref(ci)))
-    return _take(rp, ci, V.value, E.value)
+    capi.check(_L().vsgm_csr_bin_header(str(path).encode(), C.byref(V), C.byref(E)))
+    rp = np.empty(V.value + 1, np.uint64)
+    ci = np.empty(max(E.value, 1), np.uint32)
+    capi.check(_L().vsgm_read_csr_bin_into(str(path).encode(), V.value, E.value, capi.ptr(rp, C.c_uint64), capi.ptr(ci, C.c_uint32), threads))
+    return Graph(rp, ci[:E.value])
 
 
 def write_csr_bin(path, g):
@@ -157,9 +160,9 @@ def csr_defects(g):
 
 def degree_relabel(g, ascending=True, threads=0):
     """Relabel by (degree, id) rank; returns (relabelled graph, new_of_old)."""
-    perm = np.zeros(g.V, np.uint32)
-    rp = np.zeros(g.V + 1, np.uint64)
-    ci = np.zeros(max(g.E, 1), np.uint32)
+    perm = np.empty(g.V, np.uint32)  # all three are fully written by the call
+    rp = np.empty(g.V + 1, np.uint64)
+    ci = np.empty(max(g.E, 1), np.uint32)
     capi.check(_L().vsgm_degree_relabel(g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32), 1 if ascending else 0, threads,
                                         capi.ptr(perm, C.c_uint32), capi.ptr(rp, C.c_uint64), capi.ptr(ci, C.c_uint32)))
     return Graph(rp, ci[:g.E]), perm
@@ -179,10 +182,10 @@ def sources_of_bins(bins, n_bins):
 def materialize_view(g, sources, hop, root_degree=0, threads=0):
     """Full-V view CSR holding the rows of the sources' (hop-1)-neighbourhood."""
     sources = np.ascontiguousarray(sources, dtype=np.uint32)
-    vrp = np.zeros(g.V + 1, np.uint64)
+    vrp = np.empty(g.V + 1, np.uint64)  # fully written by the call
     n = C.c_uint64()
     cap = g.E
-    vci = np.zeros(max(cap, 1), np.uint32)
+    vci = np.empty(max(cap, 1), np.uint32)
     capi.check(_L().vsgm_view_materialize(g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32),
                                           capi.ptr(sources, C.c_uint32), len(sources), hop, root_degree, threads,
                                           capi.ptr(vrp, C.c_uint64), capi.ptr(vci, C.c_uint32), cap, C.byref(n)))

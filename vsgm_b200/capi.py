@@ -117,6 +117,8 @@ _SIGS = {
     "vsgm_plan_reorder": (C.c_int, [_P(Plan), _u8p, _P(Plan)]),
     "vsgm_plan_automorphisms": (C.c_uint64, [_P(Plan)]),
     "vsgm_read_csr_bin": (C.c_int, [C.c_char_p, _u64p, _u64p, _P(_u64p), _P(_u32p)]),
+    "vsgm_csr_bin_header": (C.c_int, [C.c_char_p, _u64p, _u64p]),
+    "vsgm_read_csr_bin_into": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint64, _u64p, _u32p, C.c_int]),
     "vsgm_write_csr_bin": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint64, _u64p, _u32p]),
     "vsgm_read_vbmap": (C.c_int, [C.c_char_p, C.c_uint64, _i32p, _i32p]),
     "vsgm_write_vbmap": (C.c_int, [C.c_char_p, C.c_uint64, _i32p, C.c_int32]),

@@ -94,14 +94,39 @@ uint64_t vsgm_plan_automorphisms(const vsgm_plan* p) { return p ? vsgm::automorp
 
 int vsgm_read_csr_bin(const char* path, uint64_t* V, uint64_t* E, uint64_t** row_ptrs, uint32_t** cols) {
   if (!path || !V || !E || !row_ptrs || !cols) return fail(VSGM_EINVAL, "null argument");
-  vsgm::Csr g;
   std::string err;
-  if (!vsgm::read_csr_bin(path, &g, &err)) return fail(VSGM_EIO, err);
-  *V = g.V;
-  *E = g.E();
-  *row_ptrs = export_vec(g.row_ptrs);
-  *cols = export_vec(g.cols);
-  if (!*row_ptrs || !*cols) return fail(VSGM_ENOMEM, "host allocation failed");
+  uint64_t nv = 0, ne = 0;
+  if (!vsgm::csr_bin_header(path, &nv, &ne, &err)) return fail(VSGM_EIO, err);
+  uint64_t* rp = (uint64_t*)std::malloc(sizeof(uint64_t) * (nv + 1));
+  uint32_t* ci = (uint32_t*)std::malloc(sizeof(uint32_t) * ne + 1);
+  if (!rp || !ci) {
+    std::free(rp);
+    std::free(ci);
+    return fail(VSGM_ENOMEM, "host allocation failed");
+  }
+  if (!vsgm::read_csr_bin_into(path, nv, ne, rp, ci, 0, &err)) {
+    std::free(rp);
+    std::free(ci);
+    return fail(VSGM_EIO, err);
+  }
+  *V = nv;
+  *E = ne;
+  *row_ptrs = rp;
+  *cols = ci;
+  return VSGM_OK;
+}
+
+int vsgm_csr_bin_header(const char* path, uint64_t* V, uint64_t* E) {
+  if (!path || !V || !E) return fail(VSGM_EINVAL, "null argument");
+  std::string err;
+  if (!vsgm::csr_bin_header(path, V, E, &err)) return fail(VSGM_EIO, err);
+  return VSGM_OK;
+}
+
+int vsgm_read_csr_bin_into(const char* path, uint64_t V, uint64_t E, uint64_t* row_ptrs, uint32_t* cols, int threads) {
+  if (!path || !row_ptrs || (E && !cols)) return fail(VSGM_EINVAL, "null argument");
+  std::string err;
+  if (!vsgm::read_csr_bin_into(path, V, E, row_ptrs, cols, threads, &err)) return fail(VSGM_EIO, err);
   return VSGM_OK;
 }
 

@@ -1,7 +1,10 @@
 // Host-side graph layer (see graph.hpp).
 #include "graph.hpp"
 
+#include <fcntl.h>
 #include <omp.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <atomic>
@@ -141,30 +144,82 @@ void gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t dmax
   csr_from_edges(V, src, dst, threads, out);
 }
 
-bool read_csr_bin(const std::string& path, Csr* out, std::string* err) {
-  FILE* f = std::fopen(path.c_str(), "rb");
-  if (!f) {
+bool csr_bin_header(const std::string& path, uint64_t* V, uint64_t* E, std::string* err) {
+  const int fd = ::open(path.c_str(), O_RDONLY);
+  if (fd < 0) {
     if (err) *err = "cannot open " + path;
     return false;
   }
   uint64_t hdr[4];
-  bool ok = std::fread(hdr, sizeof(uint64_t), 4, f) == 4;
-  if (ok && (hdr[0] != 4 || hdr[1] != 8)) {
-    if (err) *err = "unsupported id widths in " + path;
-    std::fclose(f);
+  struct stat st;
+  const bool got = ::pread(fd, hdr, sizeof(hdr), 0) == (ssize_t)sizeof(hdr) && ::fstat(fd, &st) == 0;
+  ::close(fd);
+  if (!got) {
+    if (err) *err = "truncated or inconsistent csr file " + path;
     return false;
   }
-  if (ok) {
-    out->V = hdr[2];
-    out->row_ptrs.resize(hdr[2] + 1);
-    out->cols.resize(hdr[3]);
-    ok = std::fread(out->row_ptrs.data(), sizeof(uint64_t), hdr[2] + 1, f) == hdr[2] + 1;
-    ok = ok && std::fread(out->cols.data(), sizeof(uint32_t), hdr[3], f) == hdr[3];
-    ok = ok && out->row_ptrs[hdr[2]] == hdr[3] && std::fgetc(f) == EOF;
+  if (hdr[0] != 4 || hdr[1] != 8) {
+    if (err) *err = "unsupported id widths in " + path;
+    return false;
   }
-  std::fclose(f);
+  // the sizes must describe the file exactly (and must not overflow doing so)
+  const uint64_t Vn = hdr[2], En = hdr[3];
+  if (Vn >= (1ull << 40) || En >= (1ull << 60) || (uint64_t)st.st_size != 32 + 8 * (Vn + 1) + 4 * En) {
+    if (err) *err = "truncated or inconsistent csr file " + path;
+    return false;
+  }
+  *V = Vn;
+  *E = En;
+  return true;
+}
+
+// read len bytes at off into dst in chunks spread over T threads
+static bool pread_all(int fd, char* dst, uint64_t off, uint64_t len, int T) {
+  const uint64_t chunk = 64ull << 20;
+  const int64_t n = (int64_t)((len + chunk - 1) / chunk);
+  std::atomic<bool> ok{true};
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1)
+  for (int64_t k = 0; k < n; k++) {
+    uint64_t a = (uint64_t)k * chunk, z = std::min<uint64_t>(len, a + chunk);
+    while (a < z && ok.load(std::memory_order_relaxed)) {
+      const ssize_t r = ::pread(fd, dst + a, z - a, (off_t)(off + a));
+      if (r <= 0) {
+        ok = false;
+        break;
+      }
+      a += (uint64_t)r;
+    }
+  }
+  return ok.load();
+}
+
+bool read_csr_bin_into(const std::string& path, uint64_t V, uint64_t E, uint64_t* row_ptrs, uint32_t* cols, int threads, std::string* err) {
+  uint64_t fv = 0, fe = 0;
+  if (!csr_bin_header(path, &fv, &fe, err)) return false;
+  if (fv != V || fe != E) {
+    if (err) *err = "csr file " + path + " does not have the expected sizes";
+    return false;
+  }
+  const int fd = ::open(path.c_str(), O_RDONLY);
+  if (fd < 0) {
+    if (err) *err = "cannot open " + path;
+    return false;
+  }
+  const int T = nthreads(threads);
+  bool ok = pread_all(fd, (char*)row_ptrs, 32, 8 * (V + 1), T) && pread_all(fd, (char*)cols, 32 + 8 * (V + 1), 4 * E, T);
+  ::close(fd);
+  ok = ok && row_ptrs[V] == E;
   if (!ok && err) *err = "truncated or inconsistent csr file " + path;
   return ok;
+}
+
+bool read_csr_bin(const std::string& path, Csr* out, std::string* err) {
+  uint64_t V = 0, E = 0;
+  if (!csr_bin_header(path, &V, &E, err)) return false;
+  out->V = V;
+  out->row_ptrs.resize(V + 1);
+  out->cols.resize(E);
+  return read_csr_bin_into(path, V, E, out->row_ptrs.data(), out->cols.data(), 0, err);
 }
 
 bool write_csr_bin(const std::string& path, const Csr& g, std::string* err) {

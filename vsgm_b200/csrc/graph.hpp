@@ -37,6 +37,12 @@ void gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t dmax
 // CSR .bin (src/graph/graph_io.h:57-100 reader, :313-339 writer layout):
 // u64 sizeof(uintV)=4, u64 sizeof(uintE)=8, u64 V, u64 E, u64 row_ptrs[V+1], u32 cols[E]
 bool read_csr_bin(const std::string& path, Csr* out, std::string* err);
+// The header alone, with the file's size checked against it exactly (the reference
+// asserts that the file ends right after the cols).
+bool csr_bin_header(const std::string& path, uint64_t* V, uint64_t* E, std::string* err);
+// row_ptrs and cols straight into caller buffers (V+1 and E entries) with parallel
+// positioned reads of large chunks: no intermediate copy, no zero fill.
+bool read_csr_bin_into(const std::string& path, uint64_t V, uint64_t E, uint64_t* row_ptrs, uint32_t* cols, int threads, std::string* err);
 bool write_csr_bin(const std::string& path, const Csr& g, std::string* err);
 
 // .vbmap (src/tools/view_packing.cc:309-322, read at src/view/view_bin_manager.h:30-67):
