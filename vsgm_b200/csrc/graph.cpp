@@ -131,15 +131,30 @@ void gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t dmax
     for (uint64_t i = 0; i < V; i++) cdf[i] /= s;
     cdf[V - 1] = 1.0;
   }
+  // Inverse-CDF sampling through a bucket index: bucket k covers r in [k/K, (k+1)/K)
+  // and idx[k] = upper_bound(cdf, k/K), so upper_bound(cdf, r) lies in
+  // [idx[k], idx[k+1]] and the short search there returns exactly what a search
+  // over the whole array would (same graphs as before, without walking a
+  // cache-missing binary search over all V entries per endpoint).
+  const uint64_t K = std::max<uint64_t>(1, std::min<uint64_t>(V, 1ull << 26));
+  auto edge_of = [K](uint64_t k) { return (double)k / (double)K; };
+  std::vector<uint64_t> idx(K + 1);
+#pragma omp parallel for num_threads(T) schedule(static)
+  for (int64_t k = 0; k <= (int64_t)K; k++) idx[k] = (uint64_t)(std::upper_bound(cdf.begin(), cdf.end(), edge_of((uint64_t)k)) - cdf.begin());
+  auto sample = [&](double r) -> uint32_t {
+    uint64_t k = (uint64_t)(r * (double)K);
+    if (k >= K) k = K - 1;
+    while (k > 0 && edge_of(k) > r) k--;
+    while (k + 1 < K && edge_of(k + 1) <= r) k++;
+    const uint64_t pos = (uint64_t)(std::upper_bound(cdf.begin() + idx[k], cdf.begin() + idx[k + 1], r) - cdf.begin());
+    return (uint32_t)(pos >= V ? V - 1 : pos);
+  };
   const uint64_t m = target_edges;
   std::vector<uint32_t> src(m), dst(m);
 #pragma omp parallel for num_threads(T) schedule(static)
   for (int64_t i = 0; i < (int64_t)m; i++) {
-    double r1 = unit_double(seed, 2 * (uint64_t)i), r2 = unit_double(seed, 2 * (uint64_t)i + 1);
-    src[i] = (uint32_t)(std::upper_bound(cdf.begin(), cdf.end(), r1) - cdf.begin());
-    dst[i] = (uint32_t)(std::upper_bound(cdf.begin(), cdf.end(), r2) - cdf.begin());
-    if (src[i] >= V) src[i] = (uint32_t)(V - 1);
-    if (dst[i] >= V) dst[i] = (uint32_t)(V - 1);
+    src[i] = sample(unit_double(seed, 2 * (uint64_t)i));
+    dst[i] = sample(unit_double(seed, 2 * (uint64_t)i + 1));
   }
   csr_from_edges(V, src, dst, threads, out);
 }
