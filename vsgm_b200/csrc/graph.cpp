@@ -29,48 +29,102 @@ double unit_double(uint64_t seed, uint64_t i) { return (double)(mix64(seed, i) >
 static int nthreads(int t) { return t > 0 ? t : omp_get_max_threads(); }
 
 void csr_from_edges(uint64_t V, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst, int threads, Csr* out) {
+  // Symmetrise, drop self loops and duplicates, sort every row.  Both copies of
+  // every edge are first partitioned by the block of 2^16 rows their source falls
+  // in (per-thread counts, no atomics), then each block is counting-sorted by row
+  // with block-local counters that stay in cache, and its rows are sorted and
+  // de-duplicated.  The result depends only on the edge set.
   const int T = nthreads(threads);
   const uint64_t m = src.size();
-  std::vector<uint64_t> deg(V + 1, 0);
+  constexpr int kShift = 16;
+  const uint64_t B = (V >> kShift) + 1;
+  auto slice = [&](int t, uint64_t* lo, uint64_t* hi) {
+    *lo = m * (uint64_t)t / (uint64_t)T;
+    *hi = m * (uint64_t)(t + 1) / (uint64_t)T;
+  };
+  std::vector<uint64_t> cnt((size_t)T * B, 0);
+#pragma omp parallel num_threads(T)
   {
-    std::atomic<uint64_t>* d = reinterpret_cast<std::atomic<uint64_t>*>(deg.data());
-#pragma omp parallel for num_threads(T) schedule(static)
-    for (int64_t i = 0; i < (int64_t)m; i++) {
-      if (src[i] == dst[i]) continue;
-      d[src[i]].fetch_add(1, std::memory_order_relaxed);
-      d[dst[i]].fetch_add(1, std::memory_order_relaxed);
-    }
-  }
-  std::vector<uint64_t> off(V + 1, 0);
-  for (uint64_t v = 0; v < V; v++) off[v + 1] = off[v] + deg[v];
-  std::vector<uint32_t> tmp(off[V]);
-  {
-    std::vector<uint64_t> cur(off.begin(), off.end() - 1);
-    std::atomic<uint64_t>* c = reinterpret_cast<std::atomic<uint64_t>*>(cur.data());
-#pragma omp parallel for num_threads(T) schedule(static)
-    for (int64_t i = 0; i < (int64_t)m; i++) {
-      uint32_t a = src[i], b = dst[i];
+    const int t = omp_get_thread_num();
+    uint64_t lo, hi;
+    slice(t, &lo, &hi);
+    uint64_t* c = cnt.data() + (size_t)t * B;
+    for (uint64_t i = lo; i < hi; i++) {
+      const uint32_t a = src[i], b = dst[i];
       if (a == b) continue;
-      tmp[c[a].fetch_add(1, std::memory_order_relaxed)] = b;
-      tmp[c[b].fetch_add(1, std::memory_order_relaxed)] = a;
+      c[a >> kShift]++;
+      c[b >> kShift]++;
     }
   }
-  // sort + unique each row in place
-  std::vector<uint64_t> kept(V + 1, 0);
-#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
-  for (int64_t v = 0; v < (int64_t)V; v++) {
-    uint32_t* b = tmp.data() + off[v];
-    uint32_t* e = tmp.data() + off[v + 1];
-    std::sort(b, e);
-    kept[v] = (uint64_t)(std::unique(b, e) - b);
+  std::vector<uint64_t> boff(B + 1, 0);
+  {
+    uint64_t run = 0;
+    for (uint64_t b = 0; b < B; b++) {
+      boff[b] = run;
+      for (int t = 0; t < T; t++) {
+        const uint64_t n = cnt[(size_t)t * B + b];
+        cnt[(size_t)t * B + b] = run;  // becomes this thread's write cursor in block b
+        run += n;
+      }
+    }
+    boff[B] = run;
   }
+  std::vector<uint64_t> pairs(boff[B]);  // (row << 32) | neighbour
+#pragma omp parallel num_threads(T)
+  {
+    const int t = omp_get_thread_num();
+    uint64_t lo, hi;
+    slice(t, &lo, &hi);
+    uint64_t* cur = cnt.data() + (size_t)t * B;
+    for (uint64_t i = lo; i < hi; i++) {
+      const uint32_t a = src[i], b = dst[i];
+      if (a == b) continue;
+      pairs[cur[a >> kShift]++] = ((uint64_t)a << 32) | b;
+      pairs[cur[b >> kShift]++] = ((uint64_t)b << 32) | a;
+    }
+  }
+  // per block: rows by counting sort, then sort + unique each row
+  std::vector<uint32_t> tmp(boff[B]);
+  std::vector<uint64_t> start(V + 1, 0), kept(V, 0), bkept(B + 1, 0);
+#pragma omp parallel num_threads(T)
+  {
+    std::vector<uint64_t> pos;
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t b = 0; b < (int64_t)B; b++) {
+      const uint64_t v0 = (uint64_t)b << kShift, v1 = std::min<uint64_t>(V, v0 + (1ull << kShift));
+      if (v0 >= v1) continue;
+      pos.assign(v1 - v0 + 1, 0);
+      for (uint64_t k = boff[b]; k < boff[b + 1]; k++) pos[(pairs[k] >> 32) - v0 + 1]++;
+      pos[0] = boff[b];
+      for (uint64_t r = 1; r <= v1 - v0; r++) pos[r] += pos[r - 1];
+      for (uint64_t r = 0; r < v1 - v0; r++) start[v0 + r] = pos[r];
+      for (uint64_t k = boff[b]; k < boff[b + 1]; k++) tmp[pos[(pairs[k] >> 32) - v0]++] = (uint32_t)pairs[k];
+      uint64_t sum = 0;
+      for (uint64_t v = v0; v < v1; v++) {
+        uint32_t* rb = tmp.data() + start[v];
+        uint32_t* re = tmp.data() + (v + 1 < v1 ? start[v + 1] : boff[b + 1]);
+        std::sort(rb, re);
+        kept[v] = (uint64_t)(std::unique(rb, re) - rb);
+        sum += kept[v];
+      }
+      bkept[b + 1] = sum;
+    }
+  }
+  for (uint64_t b = 0; b < B; b++) bkept[b + 1] += bkept[b];
   out->V = V;
   out->row_ptrs.assign(V + 1, 0);
-  for (uint64_t v = 0; v < V; v++) out->row_ptrs[v + 1] = out->row_ptrs[v] + kept[v];
-  out->cols.resize(out->row_ptrs[V]);
-#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
-  for (int64_t v = 0; v < (int64_t)V; v++)
-    std::memcpy(out->cols.data() + out->row_ptrs[v], tmp.data() + off[v], kept[v] * sizeof(uint32_t));
+  out->cols.resize(bkept[B]);
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1)
+  for (int64_t b = 0; b < (int64_t)B; b++) {
+    const uint64_t v0 = (uint64_t)b << kShift, v1 = std::min<uint64_t>(V, v0 + (1ull << kShift));
+    uint64_t at = bkept[b];
+    for (uint64_t v = v0; v < v1; v++) {
+      out->row_ptrs[v] = at;
+      std::memcpy(out->cols.data() + at, tmp.data() + start[v], kept[v] * sizeof(uint32_t));
+      at += kept[v];
+    }
+  }
+  out->row_ptrs[V] = bkept[B];
 }
 
 void gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed, int threads, Csr* out) {
