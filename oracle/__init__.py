@@ -27,7 +27,7 @@ def lib():
         if not os.path.exists(LIB):
             build()
         L = C.CDLL(LIB)
-        for name in ("oracle_count", "oracle_op_paths", "oracle_bruteforce"):
+        for name in ("oracle_count", "oracle_op_paths", "oracle_bruteforce", "oracle_c4_by_largest"):
             getattr(L, name).restype = C.c_uint64
         _lib = L
     return _lib
@@ -56,3 +56,10 @@ def bruteforce(plan, g, n_automorphisms, threads=0):
     """Injective edge-preserving maps of the pattern into g divided by |Aut(P)|."""
     return int(lib().oracle_bruteforce(C.byref(plan), C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
                                        C.c_uint64(n_automorphisms), threads))
+
+
+def c4_by_largest(g, sources=None, threads=0):
+    """4-cycles whose largest vertex is one of `sources` (all vertices by default)."""
+    src = np.arange(g.V, dtype=np.uint32) if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+    return int(lib().oracle_c4_by_largest(C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
+                                          _p(src, C.c_uint32), C.c_uint64(len(src)), threads))

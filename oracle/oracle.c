@@ -29,6 +29,10 @@
  *    maps P -> G divided by |Aut(P)|; small graphs only.
  * 3. oracle_op_paths: number of partial matches entering every op (summed over
  *    roots), used to check the engine's per-level statistics.
+ * 4. oracle_c4_by_largest: 4-cycles whose largest vertex is one of the given
+ *    sources, by pairwise neighbour intersections - the attribution the engine's
+ *    wedge-aggregation operator uses (the reference's 4-cycle plan attributes a
+ *    cycle to its smallest vertex; totals over all vertices agree).
  *
  * Parity: the reference's matching path cannot be built here (its moderngpu and
  * MPMCQueue submodules are not vendored and it needs a GPU), and the reference
@@ -325,4 +329,35 @@ uint64_t oracle_bruteforce(const vsgm_plan* p, uint64_t V, const uint64_t* rp, c
     maps += b.maps;
   }
   return n_automorphisms ? maps / n_automorphisms : 0;
+}
+
+/* 4-cycles u-v-w-v' whose largest vertex u is a source: for every pair v < v' of
+ * neighbours of u below u, the common neighbours w of v and v' below u (w != u by
+ * construction).  The opposite vertex and the pair {v, v'} fix the cycle, so each
+ * is counted once. */
+uint64_t oracle_c4_by_largest(uint64_t V, const uint64_t* rp, const uint32_t* ci, const uint32_t* sources, uint64_t n_sources, int threads) {
+  (void)V;
+  uint64_t total = 0;
+  const int T = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for num_threads(T) schedule(dynamic, 16) reduction(+ : total)
+  for (int64_t s = 0; s < (int64_t)n_sources; s++) {
+    const uint32_t u = sources[s];
+    for (uint64_t i = rp[u]; i < rp[u + 1] && ci[i] < u; i++)
+      for (uint64_t j = i + 1; j < rp[u + 1] && ci[j] < u; j++) {
+        const uint32_t v = ci[i], x = ci[j];
+        uint64_t a = rp[v], b = rp[x];
+        while (a < rp[v + 1] && b < rp[x + 1] && ci[a] < u && ci[b] < u) {
+          if (ci[a] < ci[b])
+            a++;
+          else if (ci[a] > ci[b])
+            b++;
+          else {
+            total++;
+            a++;
+            b++;
+          }
+        }
+      }
+  }
+  return total;
 }

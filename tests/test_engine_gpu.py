@@ -330,6 +330,15 @@ def test_four_cycle_aggregation_equals_plan(vs, orc, graphs):
     g = graphs["rmat8"]
     bins = (np.arange(g.V) % 3).astype(np.int32)
     assert vs.count_graph(g, [p], views=vs.sources_of_bins(bins, 3)) == [orc.count(p, g)]
+    # each view counts the cycles whose largest vertex is one of its sources
+    for heavy in (1 << 18, 0):
+        with vs.Engine(g.V, [p]) as e:
+            e.set_option("c4_heavy", heavy)
+            for src in vs.sources_of_bins(bins, 3):
+                e.reset_counts()
+                e.transfer_view(g, src)
+                e.match()
+                assert e.counts() == [orc.c4_by_largest(g, src)], heavy
 
 
 @pytest.mark.parametrize("reuse", [0, 1])

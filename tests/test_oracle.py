@@ -66,3 +66,20 @@ def test_oracle_counts_are_view_invariant(vs, orc, g):
         v = vs.materialize_view(g, src, p.hop, p.root_degree)
         total += orc.count(p, v, src)
     assert total == whole
+
+
+def test_four_cycles_by_largest_vertex(vs, orc, g):
+    """The largest-vertex attribution of 4-cycles: over all vertices it is the
+    4-cycle count (brute force), over a partition of the vertices it sums to it,
+    and on C_n / K_n it has closed forms."""
+    p = vs.plan_pattern(1)
+    for h in (g, vs.gen_chung_lu(300, 1500, 2.3, 40, seed=6), vs.degree_relabel(g)[0]):
+        total = orc.bruteforce(p, h, vs.automorphisms(p))
+        assert orc.c4_by_largest(h) == total == orc.count(p, h)
+        parts = [np.arange(b, h.V, 3, dtype=np.uint32) for b in range(3)]
+        assert sum(orc.c4_by_largest(h, s) for s in parts) == total
+    c = cycle_graph(vs, 4)
+    assert orc.c4_by_largest(c, np.array([3], np.uint32)) == 1 and orc.c4_by_largest(c, np.array([0, 1, 2], np.uint32)) == 0
+    k = complete_graph(vs, 6)  # 3 * C(6, 4) cycles; the one whose largest vertex is u: 3 * C(u, 3)
+    for u in range(6):
+        assert orc.c4_by_largest(k, np.array([u], np.uint32)) == 3 * (u * (u - 1) * (u - 2) // 6)
