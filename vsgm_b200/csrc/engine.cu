@@ -120,7 +120,7 @@ struct vsgm_engine {
     bool lane_merge = false;         // counting kernels: lane-partitioned merge
     bool c4_aggregate = true;        // 4-cycle plans: wedge aggregation instead of the op sequence
     bool set_reuse = true;           // COMPUTE o + COMPUTE_COUNT w over the same set: count pairs of one intersection
-    uint64_t c4_heavy = 1ull << 18;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
+    uint64_t c4_heavy = 1ull << 16;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
     uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
     uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
   };
@@ -695,7 +695,7 @@ struct vsgm_engine {
   // totals over all sources are the same.  Roots with at least kC4Heavy wedges
   // (most of the work on skewed graphs) go through the L2-resident group kernels,
   // the rest through k_c4_aggregate (one root per block).  Threshold: the
-  // per-plan knob c4_heavy (default 2^18 wedges).
+  // per-plan knob c4_heavy (default 2^16 wedges).
   void c4_aggregate(const uint32_t* roots, uint64_t n) {
     const int last = (int)plan->n_ops - 1;
     Mark m(arena);
