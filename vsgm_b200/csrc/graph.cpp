@@ -362,8 +362,10 @@ bool materialize_view(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t V
       in_view[s] = 1;
     }
   }
-  // breadth-first layers: a vertex at distance < hop from a kept source gets its row
+  // breadth-first layers: a vertex at distance < hop from a kept source gets its row;
+  // the last layer only marks (no frontier is needed after it)
   for (int layer = 1; layer < hop; layer++) {
+    const bool last = layer + 1 == hop;
     std::vector<std::vector<uint32_t>> next(T);
 #pragma omp parallel num_threads(T)
     {
@@ -373,18 +375,38 @@ bool materialize_view(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t V
         uint32_t x = frontier[i];
         for (uint64_t j = row_ptrs[x]; j < row_ptrs[x + 1]; j++) {
           uint32_t y = cols[j];
-          if (!__atomic_exchange_n(&in_view[y], (uint8_t)1, __ATOMIC_RELAXED)) mine.push_back(y);
+          if (__atomic_load_n(&in_view[y], __ATOMIC_RELAXED)) continue;
+          if (last)
+            __atomic_store_n(&in_view[y], (uint8_t)1, __ATOMIC_RELAXED);
+          else if (!__atomic_exchange_n(&in_view[y], (uint8_t)1, __ATOMIC_RELAXED))
+            mine.push_back(y);
         }
       }
     }
+    if (last) break;
     frontier.clear();
     for (auto& v : next) frontier.insert(frontier.end(), v.begin(), v.end());
   }
-  uint64_t total = 0;
-  for (uint64_t v = 0; v < V; v++) {
-    view_row_ptrs[v] = total;
-    if (in_view[v]) total += row_ptrs[v + 1] - row_ptrs[v];
+  // offsets: per-block sums, then the block prefix, then each block's own prefix
+  const int64_t nb = (int64_t)((V + 65535) >> 16);
+  std::vector<uint64_t> bsum(nb + 1, 0);
+#pragma omp parallel for num_threads(T) schedule(static)
+  for (int64_t b = 0; b < nb; b++) {
+    uint64_t s = 0;
+    for (uint64_t v = (uint64_t)b << 16; v < std::min<uint64_t>(V, ((uint64_t)b + 1) << 16); v++)
+      if (in_view[v]) s += row_ptrs[v + 1] - row_ptrs[v];
+    bsum[b + 1] = s;
   }
+  for (int64_t b = 0; b < nb; b++) bsum[b + 1] += bsum[b];
+#pragma omp parallel for num_threads(T) schedule(static)
+  for (int64_t b = 0; b < nb; b++) {
+    uint64_t at = bsum[b];
+    for (uint64_t v = (uint64_t)b << 16; v < std::min<uint64_t>(V, ((uint64_t)b + 1) << 16); v++) {
+      view_row_ptrs[v] = at;
+      if (in_view[v]) at += row_ptrs[v + 1] - row_ptrs[v];
+    }
+  }
+  const uint64_t total = bsum[nb];
   view_row_ptrs[V] = total;
   *n_cols = total;
   if (total > cols_cap) return false;
