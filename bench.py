@@ -84,8 +84,9 @@ def make_workload(vs, scale=22, edge_factor=16, seed=2, relabel="asc", queries=N
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
-    def __init__(self, path):
+    def __init__(self, path, device=0):
         self.path = path
+        self.device = device
         self.p = None
 
     def __enter__(self):
@@ -93,7 +94,7 @@ class Clocks:
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.f = open(self.path, "w")
-            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200", "-i", "0"],
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200", "-i", str(self.device)],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
@@ -269,8 +270,8 @@ def main():
     op_ms = {}
     op_bytes = {}
     launches = 0
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with Clocks(os.path.join(ROOT, "gpurun_out", "bench_clocks.csv")) as ck:
+    import tempfile
+    with Clocks(os.path.join(tempfile.gettempdir(), f"vsgm_bench_clocks_{os.getpid()}.csv"), device=local) as ck:
         ev0.record(stream)
         for _ in range(args.steps):
             eng.match()

@@ -1,7 +1,7 @@
 """CPU ORACLE (test infrastructure only): ctypes access to oracle/liboracle.so.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
-use this package, and only as the checker or the timed CPU baseline; the product
+use this package, and only to check results or as the timed CPU baseline; the product
 never imports it.  See oracle/oracle.c for what each function restates.
 """
 import ctypes as C

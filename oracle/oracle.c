@@ -1,7 +1,7 @@
 /* CPU ORACLE - test infrastructure only.
  *
  * Nothing in the product links, imports or executes this file.  It is used by
- * tests/ (as the checker), by __graft_entry__.smoke() and by bench.py's CPU
+ * tests/ (to check results), by __graft_entry__.smoke() and by bench.py's CPU
  * baseline / reference arm.
  *
  * 1. oracle_count: a restatement of the reference executor for one plan, one
