@@ -13,6 +13,7 @@
 #include <cstring>
 #include <fstream>
 #include <numeric>
+#include <utility>
 
 namespace vsgm {
 
@@ -28,7 +29,7 @@ double unit_double(uint64_t seed, uint64_t i) { return (double)(mix64(seed, i) >
 
 static int nthreads(int t) { return t > 0 ? t : omp_get_max_threads(); }
 
-void csr_from_edges(uint64_t V, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst, int threads, Csr* out) {
+void csr_from_edges(uint64_t V, std::vector<uint32_t>&& src, std::vector<uint32_t>&& dst, int threads, Csr* out) {
   // Symmetrise, drop self loops and duplicates, sort every row.  Both copies of
   // every edge are first partitioned by the block of 2^16 rows their source falls
   // in (per-thread counts, no atomics), then each block is counting-sorted by row
@@ -83,6 +84,10 @@ void csr_from_edges(uint64_t V, const std::vector<uint32_t>& src, const std::vec
       pairs[cur[b >> kShift]++] = ((uint64_t)b << 32) | a;
     }
   }
+  // the edge lists are consumed: release them before the next buffer (peak host
+  // memory stays at pairs + edge lists, then pairs + rows, then rows + result)
+  std::vector<uint32_t>().swap(src);
+  std::vector<uint32_t>().swap(dst);
   // per block: rows by counting sort, then sort + unique each row
   std::vector<uint32_t> tmp(boff[B]);
   std::vector<uint64_t> start(V + 1, 0), kept(V, 0), bkept(B + 1, 0);
@@ -110,6 +115,7 @@ void csr_from_edges(uint64_t V, const std::vector<uint32_t>& src, const std::vec
       bkept[b + 1] = sum;
     }
   }
+  std::vector<uint64_t>().swap(pairs);
   for (uint64_t b = 0; b < B; b++) bkept[b + 1] += bkept[b];
   out->V = V;
   out->row_ptrs.assign(V + 1, 0);
@@ -152,7 +158,7 @@ void gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t
     src[i] = (uint32_t)s;
     dst[i] = (uint32_t)d;
   }
-  csr_from_edges(V, src, dst, threads, out);
+  csr_from_edges(V, std::move(src), std::move(dst), threads, out);
 }
 
 void gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t dmax, uint64_t seed, int threads, Csr* out) {
@@ -210,7 +216,7 @@ void gen_chung_lu(uint64_t V, uint64_t target_edges, double gamma, uint64_t dmax
     src[i] = sample(unit_double(seed, 2 * (uint64_t)i));
     dst[i] = sample(unit_double(seed, 2 * (uint64_t)i + 1));
   }
-  csr_from_edges(V, src, dst, threads, out);
+  csr_from_edges(V, std::move(src), std::move(dst), threads, out);
 }
 
 bool csr_bin_header(const std::string& path, uint64_t* V, uint64_t* E, std::string* err) {

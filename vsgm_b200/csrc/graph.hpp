@@ -24,7 +24,7 @@ double unit_double(uint64_t seed, uint64_t i);
 // Build a CSR from undirected edge endpoints: self-loops dropped, both
 // directions added, duplicates removed (the rules of
 // src/preprocess/preprocess_graph.h:12-92, without dropping isolated vertices).
-void csr_from_edges(uint64_t V, const std::vector<uint32_t>& src, const std::vector<uint32_t>& dst, int threads, Csr* out);
+void csr_from_edges(uint64_t V, std::vector<uint32_t>&& src, std::vector<uint32_t>&& dst, int threads, Csr* out);
 
 // R-MAT: edge_factor * 2^scale draws, quadrant probabilities a, b, c, 1-a-b-c.
 void gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed, int threads, Csr* out);
