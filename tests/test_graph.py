@@ -113,6 +113,14 @@ def test_vbmap_round_trip(vs, tmp_path):
     p.write_text("2\n0\n5\n")
     with pytest.raises(vs.VsgmError):
         vs.read_vbmap(p, 2)
+    # Windows line ends and spare whitespace parse like the reference's operator>>
+    p.write_bytes(b"3\r\n0\r\n2 \t\n1\r\n\n")
+    got, nb = vs.read_vbmap(p, 3)
+    assert nb == 3 and got.tolist() == [0, 2, 1]
+    for bad in (b"2\n0\n-1\n", b"2\n0\nx\n", b"-2\n0\n", b"2\n0\n"):
+        p.write_bytes(bad)
+        with pytest.raises(vs.VsgmError):
+            vs.read_vbmap(p, 2)
 
 
 def _halo(g, sources, hop, root_degree):

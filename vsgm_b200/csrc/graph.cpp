@@ -312,18 +312,58 @@ bool write_csr_bin(const std::string& path, const Csr& g, std::string* err) {
   return ok;
 }
 
+// The whole file is read at once and parsed by hand: decimal integers separated by
+// whitespace, the first being the number of bins (the reference streams it with
+// operator>>, src/view/view_bin_manager.h:37-41).
+static bool next_int(const char*& p, const char* end, int64_t* out) {
+  while (p < end && (*p == ' ' || *p == '\n' || *p == '\r' || *p == '\t')) p++;
+  if (p >= end) return false;
+  bool neg = false;
+  if (*p == '-') {
+    neg = true;
+    p++;
+  }
+  if (p >= end || *p < '0' || *p > '9') return false;
+  int64_t v = 0;
+  while (p < end && *p >= '0' && *p <= '9') {
+    v = v * 10 + (*p - '0');
+    if (v > (1ll << 40)) return false;
+    p++;
+  }
+  *out = neg ? -v : v;
+  return true;
+}
+
 bool read_vbmap(const std::string& path, uint64_t V, std::vector<int32_t>* bins, int32_t* n_bins, std::string* err) {
-  std::ifstream in(path);
-  if (!in) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
     if (err) *err = "cannot open " + path;
     return false;
   }
+  std::string buf;
+  {
+    std::fseek(f, 0, SEEK_END);
+    const long n = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    buf.resize(n > 0 ? (size_t)n : 0);
+    const bool ok = n >= 0 && std::fread(&buf[0], 1, buf.size(), f) == buf.size();
+    std::fclose(f);
+    if (!ok) {
+      if (err) *err = "cannot read " + path;
+      return false;
+    }
+  }
+  const char* p = buf.data();
+  const char* end = p + buf.size();
   int64_t nb = 0;
-  in >> nb;
-  bins->assign(V, 0);
+  if (!next_int(p, end, &nb) || nb < 0 || nb > 0x7fffffff) {
+    if (err) *err = "bad bin count in " + path;
+    return false;
+  }
+  bins->resize(V);
   for (uint64_t i = 0; i < V; i++) {
     int64_t b;
-    if (!(in >> b) || b < 0 || b >= nb) {
+    if (!next_int(p, end, &b) || b < 0 || b >= nb) {
       if (err) *err = "bad or missing bin id for vertex " + std::to_string(i) + " in " + path;
       return false;
     }
@@ -334,15 +374,32 @@ bool read_vbmap(const std::string& path, uint64_t V, std::vector<int32_t>* bins,
 }
 
 bool write_vbmap(const std::string& path, const std::vector<int32_t>& bins, int32_t n_bins, std::string* err) {
-  FILE* f = std::fopen(path.c_str(), "w");
+  FILE* f = std::fopen(path.c_str(), "wb");
   if (!f) {
     if (err) *err = "cannot create " + path;
     return false;
   }
-  std::fprintf(f, "%d\n", n_bins);
-  for (int32_t b : bins) std::fprintf(f, "%d\n", b);
-  std::fclose(f);
-  return true;
+  std::string out;
+  out.reserve(12 * (bins.size() + 1));
+  auto put = [&](int64_t v) {
+    char tmp[24];
+    int n = 0;
+    bool neg = v < 0;
+    uint64_t u = neg ? (uint64_t)(-v) : (uint64_t)v;
+    do {
+      tmp[n++] = (char)('0' + u % 10);
+      u /= 10;
+    } while (u);
+    if (neg) out.push_back('-');
+    while (n) out.push_back(tmp[--n]);
+    out.push_back('\n');
+  };
+  put(n_bins);
+  for (int32_t b : bins) put(b);
+  bool ok = std::fwrite(out.data(), 1, out.size(), f) == out.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok && err) *err = "write failed for " + path;
+  return ok;
 }
 
 uint64_t csr_defects(const Csr& g) {
