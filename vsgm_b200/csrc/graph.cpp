@@ -482,14 +482,16 @@ bool materialize_view(const uint64_t* row_ptrs, const uint32_t* cols, uint64_t V
 void degree_relabel(const Csr& g, bool ascending, int threads, std::vector<uint32_t>* new_of_old, Csr* out) {
   const int T = nthreads(threads);
   const uint64_t V = g.V;
-  std::vector<uint32_t> order(V);
-  for (uint64_t v = 0; v < V; v++) order[v] = (uint32_t)v;
   auto deg = [&](uint32_t v) { return g.row_ptrs[v + 1] - g.row_ptrs[v]; };
-  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-    uint64_t da = deg(a), db = deg(b);
-    if (da != db) return ascending ? da < db : da > db;
-    return a < b;
-  });
+  // rank by (degree, id): a counting sort over degrees, ids ascending inside each
+  // degree (the order a stable sort by degree gives)
+  uint64_t dmax = 0;
+  for (uint64_t v = 0; v < V; v++) dmax = std::max<uint64_t>(dmax, deg((uint32_t)v));
+  std::vector<uint64_t> at(dmax + 2, 0);
+  for (uint64_t v = 0; v < V; v++) at[(ascending ? deg((uint32_t)v) : dmax - deg((uint32_t)v)) + 1]++;
+  for (uint64_t d = 0; d <= dmax; d++) at[d + 1] += at[d];
+  std::vector<uint32_t> order(V);
+  for (uint64_t v = 0; v < V; v++) order[at[ascending ? deg((uint32_t)v) : dmax - deg((uint32_t)v)]++] = (uint32_t)v;
   new_of_old->assign(V, 0);
   for (uint64_t r = 0; r < V; r++) (*new_of_old)[order[r]] = (uint32_t)r;
   out->V = V;
