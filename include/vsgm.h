@@ -244,6 +244,9 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   gallop);
  *   "lane_slice" (default 16): in the fused tail a child whose slice of the staged
  *   set is at most this long is handled by one lane, longer ones by the whole warp;
+ *   "tail_merge" (default 0): in the fused tail a heavy child intersects its slice
+ *   and its part of N(c) by a merge-path split over the warp's lanes instead of
+ *   the walk / gallop (experimental: not yet timed);
  *   "c4_heavy" (default 2^16): roots with at least this many wedges are counted by
  *   groups sharing the whole GPU with L2-resident counters (0: every root);
  *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT

@@ -123,6 +123,7 @@ struct vsgm_engine {
     uint64_t c4_heavy = 1ull << 16;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
     uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
     uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
+    bool tail_merge = false;           // fused tail: heavy children by a merge-path split over the lanes
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -608,13 +609,18 @@ struct vsgm_engine {
     begin_op();
     const unsigned g = grid_warps(f.P);
     const bool other = fd.other >= 0;
+    const bool merge = cur.tail_merge;
     switch (fd.known.nb) {
-#define VSGM_FUSED(NK)                                                                    \
-  case NK:                                                                                \
-    if (other)                                                                            \
-      k_mat_count<NK, true><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes);  \
-    else                                                                                  \
-      k_mat_count<NK, false><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes); \
+#define VSGM_FUSED(NK)                                                                          \
+  case NK:                                                                                      \
+    if (other && merge)                                                                         \
+      k_mat_count<NK, true, true><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes);  \
+    else if (other)                                                                             \
+      k_mat_count<NK, true><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes);        \
+    else if (merge)                                                                             \
+      k_mat_count<NK, false, true><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes); \
+    else                                                                                        \
+      k_mat_count<NK, false><<<g, 256, 0, stream>>>(f, fd, d_rp, d_ci, d_total, d_bytes);       \
     break;
       VSGM_FUSED(1)
       VSGM_FUSED(2)
@@ -1372,6 +1378,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   }
   if (n == "c4_aggregate") {
     for (int k = lo; k < hi; k++) e->knobs[k].c4_aggregate = value != 0;
+    return VSGM_OK;
+  }
+  if (n == "tail_merge") {
+    for (int k = lo; k < hi; k++) e->knobs[k].tail_merge = value != 0;
     return VSGM_OK;
   }
   if (n == "lane_slice") {

@@ -576,7 +576,10 @@ __device__ __forceinline__ void child_slice(const FusedDesc& fd, const Window& w
   *ib = (hi <= 0xffffffffull) ? smem_lower_bound(I, *ia, ni, hi) : ni;
 }
 
-template <int NK, bool kOther>
+// kMergeTail: heavy children intersect their slice and their part of N(c) by a
+// merge-path split over the 32 lanes (each lane binary-searches its diagonal, then
+// merges its share) instead of the walk / gallop of the default instantiation.
+template <int NK, bool kOther, bool kMergeTail = false>
 __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
                                                    unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
   __shared__ uint32_t stage[8][kStageCap];
@@ -669,6 +672,38 @@ __global__ void __launch_bounds__(256, 3) k_mat_count(Frame f, FusedDesc fd, con
           if (s2 >= e2) continue;
           const uint32_t excl = excl_child ? c : 0xffffffffu;
           uint64_t ocur = 0;
+          if (kMergeTail) {
+            // A = I[ia, ib) (stage), B = ci[s2, e2); every match is counted by the
+            // lane that takes its A element (A goes first on ties)
+            const uint64_t na = ib - ia, nb = e2 - s2, tot = na + nb;
+            const uint64_t per = (tot + kWarp - 1) / kWarp;
+            const uint64_t d0 = (uint64_t)lane * per < tot ? (uint64_t)lane * per : tot;
+            const uint64_t d1 = d0 + per < tot ? d0 + per : tot;
+            if (d0 < d1) {
+              uint64_t lo = d0 > nb ? d0 - nb : 0, hi = d0 < na ? d0 : na;
+              while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (I[ia + mid] <= __ldg(ci + s2 + (d0 - 1 - mid)))
+                  lo = mid + 1;
+                else
+                  hi = mid;
+              }
+              uint64_t i = lo, j = d0 - lo;
+              for (uint64_t step = d0; step < d1; step++) {
+                if (i < na) {
+                  const uint32_t a = I[ia + i];
+                  const uint32_t b = j < nb ? __ldg(ci + s2 + j) : 0u;
+                  if (j >= nb || a <= b) {
+                    if (j < nb && a == b && a != excl) acc += kOther ? count_vs(oset, on, &ocur, a, fd.other_op) : 1ull;
+                    i++;
+                    continue;
+                  }
+                }
+                j++;
+              }
+            }
+            continue;
+          }
           // walk N(c)'s part coalesced, probing the stage, unless it is much longer than the slice
           if ((uint64_t)(ib - ia) * fd.walk_ratio < (e2 - s2)) {
             uint64_t cur = s2;
