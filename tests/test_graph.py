@@ -228,3 +228,24 @@ def test_engine_create_fails_cleanly_without_gpu(vs):
     p = vs.plan_clique(3)
     with pytest.raises(vs.VsgmError):
         vs.Engine(16, [p])
+
+
+def test_pm_pipeline_fails_cleanly_without_gpu(vs, tmp_path):
+    """With no usable GPU the driver reports the error and exits non-zero instead
+    of hanging its producer/consumer threads (every -gv mode)."""
+    import subprocess
+
+    import torch
+
+    from vsgm_b200 import build
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    g = vs.gen_rmat(7, 8, seed=2)
+    path = tmp_path / "g.bin"
+    vs.write_csr_bin(path, g)
+    vs.write_vbmap(str(path) + ".2.hop.vbmap", (np.arange(g.V) % 3).astype(np.int32), 3)
+    for gv in ("0", "1", "2"):
+        out = subprocess.run([build.DRIVER, "-f", str(path), "-kc", "3", "-pn", "2", "-qs", "1", "-gv", gv],
+                             capture_output=True, text=True, timeout=120)
+        assert out.returncode != 0
+        assert "error" in out.stderr
