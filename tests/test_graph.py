@@ -249,3 +249,7 @@ def test_pm_pipeline_fails_cleanly_without_gpu(vs, tmp_path):
                              capture_output=True, text=True, timeout=120)
         assert out.returncode != 0
         assert "error" in out.stderr
+    # without a partition file the driver uses one bin of every vertex
+    os.remove(str(path) + ".2.hop.vbmap")
+    out = subprocess.run([build.DRIVER, "-f", str(path), "-kc", "3"], capture_output=True, text=True, timeout=120)
+    assert "one view bin of every vertex" in out.stdout and "loaded view bin partition file, 1 view bins" in out.stdout

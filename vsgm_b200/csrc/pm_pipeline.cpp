@@ -11,7 +11,7 @@
 // -gv 0 producers materialise the halos on the host into a bounded queue of
 // host buffers, as the reference does, and each consumer uploads them.
 // Either way one consumer per GPU matches every plan and accumulates exact
-// counts.  Prints "total count for query i: N" and
+// counts.  Without a .vbmap file every vertex is a source of one bin.  Prints "total count for query i: N" and
 // "finish total time, elapsed_time=Xms" like the reference.
 #include <sys/stat.h>
 #include <sys/time.h>
@@ -151,7 +151,15 @@ int main(int argc, char** argv) {
   std::string vbmap = a.file + "." + std::to_string(hop) + ".hop.vbmap";
   std::vector<int32_t> bins(V);
   int32_t n_bins = 0;
-  if (vsgm_read_vbmap(vbmap.c_str(), V, bins.data(), &n_bins)) return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+  struct stat vb_st;
+  if (::stat(vbmap.c_str(), &vb_st) != 0) {
+    // no partition file: one bin holding every source (what view_packing produces
+    // when the whole graph fits the budget)
+    std::printf("no %s: one view bin of every vertex\n", vbmap.c_str());
+    n_bins = 1;
+  } else if (vsgm_read_vbmap(vbmap.c_str(), V, bins.data(), &n_bins)) {
+    return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+  }
   std::vector<std::vector<uint32_t>> pool(n_bins);
   for (uint64_t v = 0; v < V; v++) pool[bins[v]].push_back((uint32_t)v);
   pool.erase(std::remove_if(pool.begin(), pool.end(), [](const std::vector<uint32_t>& s) { return s.empty(); }), pool.end());
