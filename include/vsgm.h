@@ -283,7 +283,10 @@ const char* vsgm_engine_error(vsgm_engine* e);
  * file-scope device array, which every GPU that loads this library holds until the
  * process exits.  It calls no cudaMalloc or cudaFree.  The first call on a device
  * looks up the array's device address (make that first call before any stream
- * capture).  Limit: plan ops x the view's maximum degree <= 24,319; larger views
+ * capture); the address is kept per device together with the id of the context
+ * it belongs to, and looked up again when the device's context has changed (after
+ * cudaDeviceReset, the rebuilt context loads the array anew, possibly elsewhere), so
+ * the first call after such a reset also belongs before any capture.  Limit: plan ops x the view's maximum degree <= 24,319; larger views
  * are rejected with VSGM_EINVAL and a message.  The array is shared by every call on
  * the device and keeps the last call's contents (each call clears what it needs):
  * calls that overlap on the GPU race, so serialise them.  stream may be NULL (the

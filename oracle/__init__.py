@@ -16,18 +16,23 @@ _lib = None
 
 
 def build():
+    """The oracle library; with VSGM_REFERENCE set to a checkout of the reference,
+    also the harnesses compiled from its sources (oracle/_ref).  Without the
+    variable the reference is treated as absent."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref = os.environ.get("VSGM_REFERENCE", "")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
-            build()
+        # make is incremental: this rebuilds only a library older than its source
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
         L = C.CDLL(LIB)
-        for name in ("oracle_count", "oracle_op_paths", "oracle_bruteforce", "oracle_c4_by_largest"):
+        for name in ("oracle_count", "oracle_op_paths", "oracle_bruteforce", "oracle_c4_by_largest", "oracle_c4_by_largest_wedges",
+                     "oracle_cliques_by_smallest"):
             getattr(L, name).restype = C.c_uint64
         _lib = L
     return _lib
@@ -63,3 +68,18 @@ def c4_by_largest(g, sources=None, threads=0):
     src = np.arange(g.V, dtype=np.uint32) if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
     return int(lib().oracle_c4_by_largest(C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
                                           _p(src, C.c_uint32), C.c_uint64(len(src)), threads))
+
+
+def c4_by_largest_wedges(g, sources=None, threads=0):
+    """c4_by_largest by wedge counting (cost ~ wedges below each source, not pairs)."""
+    src = np.arange(g.V, dtype=np.uint32) if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+    return int(lib().oracle_c4_by_largest_wedges(C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
+                                                 _p(src, C.c_uint32), C.c_uint64(len(src)), threads))
+
+
+def cliques_by_smallest(k, g, sources=None, threads=0):
+    """k-cliques whose smallest vertex is one of `sources` (all vertices by default):
+    the per-root attribution of the clique plans, counted by definition."""
+    src = np.arange(g.V, dtype=np.uint32) if sources is None else np.ascontiguousarray(sources, dtype=np.uint32)
+    return int(lib().oracle_cliques_by_smallest(k, C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32),
+                                                _p(src, C.c_uint32), C.c_uint64(len(src)), threads))

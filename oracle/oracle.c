@@ -33,6 +33,11 @@
  *    sources, by pairwise neighbour intersections - the attribution the engine's
  *    wedge-aggregation operator uses (the reference's 4-cycle plan attributes a
  *    cycle to its smallest vertex; totals over all vertices agree).
+ *    oracle_c4_by_largest_wedges: the same count by wedge counting, fast enough
+ *    for hub roots of the full-size graphs; pinned to the pairwise form.
+ * 5. oracle_cliques_by_smallest: k-cliques whose smallest vertex is a source, by
+ *    definition (ordered candidate sets) - the clique plans' per-root attribution,
+ *    fast on hub roots; pinned to oracle_count root by root.
  *
  * Parity: the reference's matching path cannot be built here (its moderngpu and
  * MPMCQueue submodules are not vendored and it needs a GPU), and the reference
@@ -358,6 +363,99 @@ uint64_t oracle_c4_by_largest(uint64_t V, const uint64_t* rp, const uint32_t* ci
           }
         }
       }
+  }
+  return total;
+}
+
+/* The same count by wedge aggregation, for roots whose neighbourhoods are too large
+ * for the pairwise form: for a source u, L[w] = number of wedges u-v-w with
+ * v, w < u (w != u), and the cycles closed at u are sum_w C(L[w], 2) - a pair of
+ * distinct wedge centres v, v' through the same opposite vertex w.  One dense
+ * counter array per thread, reset through the list of the ids it touched.
+ * tests/test_oracle.py pins it to oracle_c4_by_largest on small graphs. */
+uint64_t oracle_c4_by_largest_wedges(uint64_t V, const uint64_t* rp, const uint32_t* ci, const uint32_t* sources, uint64_t n_sources, int threads) {
+  uint64_t total = 0;
+  const int T = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel num_threads(T) reduction(+ : total)
+  {
+    uint32_t* L = (uint32_t*)calloc(V ? V : 1, sizeof(uint32_t));
+    uint32_t* touched = (uint32_t*)malloc((V ? V : 1) * sizeof(uint32_t));
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t s = 0; s < (int64_t)n_sources; s++) {
+      const uint32_t u = sources[s];
+      uint64_t nt = 0;
+      for (uint64_t i = rp[u]; i < rp[u + 1] && ci[i] < u; i++) {
+        const uint32_t v = ci[i];
+        for (uint64_t j = rp[v]; j < rp[v + 1] && ci[j] < u; j++)
+          if (L[ci[j]]++ == 0) touched[nt++] = ci[j];
+      }
+      for (uint64_t k = 0; k < nt; k++) {
+        const uint64_t c = L[touched[k]];
+        total += c * (c - 1) / 2;
+        L[touched[k]] = 0;
+      }
+    }
+    free(L);
+    free(touched);
+  }
+  return total;
+}
+
+/* ---------------------------------------------------------------- rooted cliques */
+/* k-cliques whose smallest vertex is a source - the attribution of the reference's
+ * clique plans, whose order conditions chain v0 < v1 < ... < v(k-1)
+ * (src/query/clique.h with the partial order of src/query/partial_order.h).  An
+ * independent count, by definition rather than by the plan: candidates at each
+ * depth are the previous set's members above the vertex just chosen that are also
+ * its neighbours, found by a merge that starts both lists at the first value above
+ * that vertex (so hub rows are never walked in full).  tests/test_oracle.py pins it
+ * to oracle_count on the clique plans, root by root. */
+static uint64_t clique_rec(const uint64_t* rp, const uint32_t* ci, const uint32_t* S, uint64_t n, int left, uint32_t* bufs) {
+  /* S: sorted candidates (all adjacent to every chosen vertex); left: vertices
+   * still to choose from S */
+  if (left == 1) return n;
+  uint64_t total = 0;
+  uint32_t* out = bufs;
+  for (uint64_t a = 0; a + 1 < n; a++) {
+    const uint32_t x = S[a];
+    const uint32_t* N = ci + rp[x];
+    const uint64_t dn = rp[x + 1] - rp[x];
+    uint64_t j = lower_bound_u32(N, dn, x + 1), i = a + 1, m = 0;
+    while (i < n && j < dn) {
+      if (S[i] < N[j])
+        i++;
+      else if (S[i] > N[j])
+        j++;
+      else {
+        out[m++] = S[i];
+        i++;
+        j++;
+      }
+    }
+    if (m >= (uint64_t)(left - 1)) total += clique_rec(rp, ci, out, m, left - 1, bufs + m);
+  }
+  return total;
+}
+
+uint64_t oracle_cliques_by_smallest(int k, uint64_t V, const uint64_t* rp, const uint32_t* ci, const uint32_t* sources, uint64_t n_sources,
+                                    int threads) {
+  if (k < 2) return 0;
+  const uint64_t dmax = max_degree(V, rp) + 1;
+  uint64_t total = 0;
+  const int T = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel num_threads(T) reduction(+ : total)
+  {
+    /* one buffer of dmax per depth, handed out as a stack */
+    uint32_t* bufs = (uint32_t*)malloc((size_t)k * dmax * sizeof(uint32_t));
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t s = 0; s < (int64_t)n_sources; s++) {
+      const uint32_t v = sources[s];
+      const uint32_t* N = ci + rp[v];
+      const uint64_t dn = rp[v + 1] - rp[v];
+      const uint64_t a = lower_bound_u32(N, dn, v + 1);
+      total += clique_rec(rp, ci, N + a, dn - a, k - 1, bufs);
+    }
+    free(bufs);
   }
   return total;
 }

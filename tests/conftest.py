@@ -25,7 +25,7 @@ def vs():
 @pytest.fixture(scope="session")
 def orc():
     import oracle
-    oracle.build() if not os.path.exists(oracle.LIB) else None
+    oracle.lib()  # builds (incrementally) and loads the oracle library
     return oracle
 
 

@@ -125,7 +125,8 @@ def test_pm_pipeline_driver(vs, orc, graphs, tmp_path):
     vs.write_csr_bin(path, g)
     bins = (np.arange(g.V) * 7 % 3).astype(np.int32)
     vs.write_vbmap(str(path) + ".2.hop.vbmap", bins, 3)
-    for args, plan in [(["-kc", "4"], vs.plan_clique(4)), (["-p", "4"], vs.plan_pattern(4))]:
+    for args, plan in [(["-kc", "4"], vs.plan_clique(4)), (["-p", "4"], vs.plan_pattern(4)), (["-kc", "4", "-rl", "0"], vs.plan_clique(4)),
+                       (["-p", "1", "-rl", "0"], vs.plan_pattern(1)), (["-p", "2", "-gv", "0"], vs.plan_pattern(2))]:
         out = subprocess.run([build.DRIVER, "-f", str(path), "-m", "1", "-t", "2", "-qs", "2", "-pn", "2", "-cn", "1", "-ds", "1"] + args,
                              capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr
@@ -221,6 +222,23 @@ def test_fused_tail_large_staged_sets(vs, orc, graphs):
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
                 e.match()
                 assert e.counts() == want, cap
+
+
+@pytest.mark.parametrize("gname", ["rmat8", "chunglu", "hub"])
+def test_tail_merge_matches_oracle(vs, orc, graphs, gname):
+    """The merge-path split of heavy children in the fused tail (knob tail_merge):
+    every preset, clique and graphlet, with every child sent to the heavy pass
+    (lane_slice 0) and with the default split, equals the oracle."""
+    g = vs.degree_relabel(_hub_graph(vs))[0] if gname == "hub" else graphs[gname]
+    plans = [p for _, p in all_plans(vs)]
+    want = [orc.count(p, g) for p in plans]
+    for ls in (0, 16):
+        with vs.Engine(g.V, plans) as e:
+            e.set_option("tail_merge", 1)
+            e.set_option("lane_slice", ls)
+            e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+            e.match()
+            assert e.counts() == want, ls
 
 
 def test_relabelled_graph_same_counts(vs, orc, graphs):

@@ -249,7 +249,17 @@ def test_pm_pipeline_fails_cleanly_without_gpu(vs, tmp_path):
                              capture_output=True, text=True, timeout=120)
         assert out.returncode != 0
         assert "error" in out.stderr
-    # without a partition file the driver uses one bin of every vertex
-    os.remove(str(path) + ".2.hop.vbmap")
+    # a partition file that exists but cannot be read is an error, not a fallback
+    vb = str(path) + ".2.hop.vbmap"
+    os.remove(vb)
+    os.mkdir(vb)
     out = subprocess.run([build.DRIVER, "-f", str(path), "-kc", "3"], capture_output=True, text=True, timeout=120)
-    assert "one view bin of every vertex" in out.stdout and "loaded view bin partition file, 1 view bins" in out.stdout
+    assert out.returncode != 0 and "error" in out.stderr and "one view bin of every vertex" not in out.stdout
+    os.rmdir(vb)
+    # without a partition file the driver uses one bin of every vertex, and says so
+    out = subprocess.run([build.DRIVER, "-f", str(path), "-kc", "3"], capture_output=True, text=True, timeout=120)
+    assert "no view bin partition file" in out.stdout and "one view bin of every vertex" in out.stdout
+    assert "loaded view bin partition file" not in out.stdout
+    # ... and a halo of the whole graph (-gv 0 / 1) must fit the -m budget
+    out = subprocess.run([build.DRIVER, "-f", str(path), "-kc", "3", "-gv", "0", "-m", "1e-9"], capture_output=True, text=True, timeout=120)
+    assert out.returncode != 0 and "exceeds -m" in out.stderr

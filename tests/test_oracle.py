@@ -83,3 +83,32 @@ def test_four_cycles_by_largest_vertex(vs, orc, g):
     k = complete_graph(vs, 6)  # 3 * C(6, 4) cycles; the one whose largest vertex is u: 3 * C(u, 3)
     for u in range(6):
         assert orc.c4_by_largest(k, np.array([u], np.uint32)) == 3 * (u * (u - 1) * (u - 2) // 6)
+
+
+def test_four_cycle_wedge_oracle_equals_pairwise(vs, orc, g):
+    """The wedge-counting form of the largest-vertex 4-cycle count (used on hub roots
+    of the full-size graphs) equals the pairwise form root by root."""
+    hub = complete_graph(vs, 8)
+    for h in (g, vs.gen_chung_lu(400, 2400, 2.2, 80, seed=9), vs.degree_relabel(g)[0], hub, cycle_graph(vs, 4)):
+        for v in range(h.V):
+            s = np.array([v], np.uint32)
+            assert orc.c4_by_largest_wedges(h, s) == orc.c4_by_largest(h, s), v
+        assert orc.c4_by_largest_wedges(h) == orc.c4_by_largest(h)
+
+
+def test_rooted_clique_oracle_equals_plan_oracle(vs, orc, g):
+    """Cliques counted by definition at their smallest vertex equal the clique plans'
+    per-root counts (the plans chain v0 < v1 < ... by their order conditions), and
+    closed forms on K_n: the cliques whose smallest vertex is u number C(n-1-u, k-1)."""
+    from math import comb
+    for h in (g, vs.gen_chung_lu(400, 2400, 2.2, 80, seed=9), vs.degree_relabel(g)[0], vs.degree_relabel(g, ascending=False)[0]):
+        for k in (3, 4, 5):
+            p = vs.plan_clique(k)
+            for v in range(0, h.V, 7):
+                s = np.array([v], np.uint32)
+                assert orc.cliques_by_smallest(k, h, s) == orc.count(p, h, s), (k, v)
+            assert orc.cliques_by_smallest(k, h) == orc.count(p, h)
+    kn = complete_graph(vs, 8)
+    for k in (3, 4, 5, 6, 7):
+        for u in range(8):
+            assert orc.cliques_by_smallest(k, kn, np.array([u], np.uint32)) == comb(7 - u, k - 1)

@@ -14,6 +14,7 @@
 //     recomputing write pass, src/gpu/gpu_utils_gpsm_bin_search.h:134-171);
 //   - every count is an exact uint64 accumulated on the device and read once
 //     per match.
+#include <cuda.h>  // CUcontext / CUresult types only: driver calls go through cudaGetDriverEntryPointByVersion
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1588,9 +1589,39 @@ static_assert(kNoAllocWarpU32 == 24319, "the documented limit (plan ops x max de
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 // device address of g_noalloc_scratch per device (the host-side symbol is not a
-// device address; cudaGetSymbolAddress gives the real one)
+// device address; cudaGetSymbolAddress gives the real one), with the id of the
+// context it was looked up in: a context that is torn down and rebuilt (for
+// example after cudaDeviceReset) loads the module again, and the array may then
+// sit at another address
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_ptr[128] = {};
+unsigned long long g_noalloc_ctx[128] = {};
+
+// Unique id of the calling thread's current context (ids are never reused within
+// a process), or 0 when the driver cannot tell.  The driver calls are reached
+// through the runtime's entry-point query so that the library does not link
+// against the driver library itself.
+unsigned long long current_context_id() {
+  typedef CUresult (*GetCurrent)(CUcontext*);
+  typedef CUresult (*GetId)(CUcontext, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_current = (GetCurrent)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+      get_id = (GetId)f;
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 struct NoAllocCounters {
   unsigned long long head;
@@ -1638,9 +1669,13 @@ extern "C" int vsgm_count_noalloc(int device, const vsgm_plan* plan, uint64_t V,
     unsigned char* base = nullptr;
     {
       std::lock_guard<std::mutex> lock(g_noalloc_mu);
-      if (!g_noalloc_ptr[device]) {
-        // once per device, with that device current
+      // once per device (and again whenever the device's context has changed), with
+      // that device current; an unknown context id (0) means: look up every call
+      const unsigned long long ctx = current_context_id();
+      if (!g_noalloc_ptr[device] || ctx == 0 || ctx != g_noalloc_ctx[device]) {
+        g_noalloc_ptr[device] = nullptr;
         CK(cudaGetSymbolAddress((void**)&g_noalloc_ptr[device], g_noalloc_scratch));
+        g_noalloc_ctx[device] = ctx;
       }
       base = g_noalloc_ptr[device];
     }

@@ -3,6 +3,7 @@
 //
 //   pm_pipeline -f <graph.bin> [-m GB] [-p P | -kc k | -km k] [-t threads] [-qs queue]
 //               [-pn producers] [-cn consumers] [-dm 0|1] [-df 0|1] [-dr 0|1] [-ds 0|1] [-dst n] [-gv 0|1|2]
+//               [-rl 0|1]
 //
 // With -gv 2 (default) every consumer keeps the whole graph on its GPU and
 // matches each view bin's sources over it directly (vsgm_graph_view, no halo
@@ -11,13 +12,19 @@
 // -gv 0 producers materialise the halos on the host into a bounded queue of
 // host buffers, as the reference does, and each consumer uploads them.
 // Either way one consumer per GPU matches every plan and accumulates exact
-// counts.  Without a .vbmap file every vertex is a source of one bin.  Prints "total count for query i: N" and
-// "finish total time, elapsed_time=Xms" like the reference.
+// counts.  Without a .vbmap file (the file does not exist) every vertex is a source
+// of one bin; any other failure to open it is an error.  With -rl 1 (default) the
+// graph and its bins are relabelled so that ids ascend with degree before any view
+// is built (inside the timed region): the plans' order conditions then cut every
+// adjacency window short, and exact totals do not depend on the labelling.  Prints
+// "total count for query i: N" and "finish total time, elapsed_time=Xms" like the
+// reference.
 #include <sys/stat.h>
 #include <sys/time.h>
 
 #include <algorithm>
 #include <atomic>
+#include <cerrno>
 #include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
@@ -35,7 +42,7 @@ namespace {
 struct Args {
   std::string file = "./data/com-friendster.ungraph.txt.bin";
   double mem = 10;
-  int pattern = 1, kc = 0, km = 0, threads = 1, qs = 1, pn = 1, cn = 1, dm = 1, df = 1, dr = 0, ds = 0, dst = 1, gv = 2;
+  int pattern = 1, kc = 0, km = 0, threads = 1, qs = 1, pn = 1, cn = 1, dm = 1, df = 1, dr = 0, ds = 0, dst = 1, gv = 2, rl = 1;
 };
 
 // CommandLine's linear scan (src/common/command_line.h:32-86)
@@ -115,6 +122,7 @@ int main(int argc, char** argv) {
   if (auto v = opt(argc, argv, "-ds")) a.ds = std::atoi(v);
   if (auto v = opt(argc, argv, "-dst")) a.dst = std::atoi(v);
   if (auto v = opt(argc, argv, "-gv")) a.gv = std::atoi(v);
+  if (auto v = opt(argc, argv, "-rl")) a.rl = std::atoi(v);
   if (a.qs < a.cn || a.pn < 1 || a.cn < 1) {
     std::fprintf(stderr, "error: need -qs >= -cn >= 1 and -pn >= 1\n");
     return 1;
@@ -152,13 +160,40 @@ int main(int argc, char** argv) {
   std::vector<int32_t> bins(V);
   int32_t n_bins = 0;
   struct stat vb_st;
+  bool have_vbmap = true;
   if (::stat(vbmap.c_str(), &vb_st) != 0) {
+    if (errno != ENOENT) return std::fprintf(stderr, "error: cannot stat %s: %s\n", vbmap.c_str(), std::strerror(errno)), 1;
     // no partition file: one bin holding every source (what view_packing produces
-    // when the whole graph fits the budget)
-    std::printf("no %s: one view bin of every vertex\n", vbmap.c_str());
+    // when the whole graph fits the budget).  A halo built from it is the whole
+    // graph, so with -gv 0 / 1 it must fit the -m budget.
+    if (a.gv != 2 && 4.0 * (double)E > a.mem * 1e9)
+      return std::fprintf(stderr, "error: no %s, and one view of the whole graph (%.2f GB of adjacency) exceeds -m %g\n", vbmap.c_str(),
+                          4.0 * (double)E / 1e9, a.mem),
+             1;
+    std::printf("no view bin partition file %s: one view bin of every vertex\n", vbmap.c_str());
+    have_vbmap = false;
     n_bins = 1;
+  } else if (!S_ISREG(vb_st.st_mode)) {
+    return std::fprintf(stderr, "error: %s is not a regular file\n", vbmap.c_str()), 1;
   } else if (vsgm_read_vbmap(vbmap.c_str(), V, bins.data(), &n_bins)) {
     return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+  }
+  double t0 = now_us();
+  if (a.rl) {
+    // ids ascending with degree; the bins follow their vertices
+    std::vector<uint32_t> new_of_old(V);
+    uint64_t* rp2 = (uint64_t*)std::malloc(sizeof(uint64_t) * (V + 1));
+    uint32_t* ci2 = (uint32_t*)std::malloc(sizeof(uint32_t) * std::max<uint64_t>(E, 1));
+    if (!rp2 || !ci2) return std::fprintf(stderr, "error: host allocation failed (relabel)\n"), 1;
+    if (vsgm_degree_relabel(V, rp, ci, 1, a.threads > 1 ? a.threads : 0, new_of_old.data(), rp2, ci2))
+      return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
+    vsgm_free(rp);
+    vsgm_free(ci);
+    rp = rp2;
+    ci = ci2;
+    std::vector<int32_t> moved(V);
+    for (uint64_t v = 0; v < V; v++) moved[new_of_old[v]] = bins[v];
+    bins.swap(moved);
   }
   std::vector<std::vector<uint32_t>> pool(n_bins);
   for (uint64_t v = 0; v < V; v++) pool[bins[v]].push_back((uint32_t)v);
@@ -188,7 +223,7 @@ int main(int argc, char** argv) {
   }
   if (a.dr || a.ds)
     std::stable_sort(pool.begin(), pool.end(), [&](const auto& x, const auto& y) { return work_of(x, rp) > work_of(y, rp); });
-  std::printf("loaded view bin partition file, %zu view bins\n", pool.size());
+  if (have_vbmap) std::printf("loaded view bin partition file, %zu view bins\n", pool.size());
 
   const uint64_t cap = std::min<uint64_t>(E, (uint64_t)(a.mem * 1e9 / sizeof(uint32_t)));
   Queue q(a.qs);
@@ -196,7 +231,6 @@ int main(int argc, char** argv) {
   std::atomic<int> failed{0};
   std::vector<std::vector<uint64_t>> counts(a.cn, std::vector<uint64_t>(plans.size(), 0));
 
-  double t0 = now_us();
   std::vector<std::thread> producers, consumers;
   for (int p = 0; p < a.pn; p++)
     producers.emplace_back([&] {
