@@ -12,7 +12,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 # whole-graph totals of the R-MAT scale-22 workload (-kc 4, -p 1, -p 2); the same
-# under native, degree-ascending and degree-descending ids
+# under native, degree-ascending and degree-descending ids.  A regression guard
+# only: the engine produced them; the parity evidence is the root-sample tests.
 C2_COUNTS = [124_023_930_675, 3_848_799_057_616, 3_080_671_377_357]
 
 
@@ -58,6 +59,48 @@ def test_c2_root_sample_against_oracle(vs, orc, rmat22):
             e.match()
             got = e.counts()
         assert got == [orc.count(p, g, src) for p in chosen]
+
+
+def hub_sample(g, seed=21):
+    """Roots that reach every heavy path of the operators the bench times: the 64
+    highest-degree vertices (heavy-root groups of the 4-cycle aggregation, hub lists
+    of the diamond and the 4-clique), the 16 largest out-neighbourhoods (neighbours
+    above the vertex) plus every 500th of the next 20,000 (the widest staged sets and
+    heavy children of the 4-clique tail), and 500 random roots (the light paths)."""
+    deg = g.degrees()
+    rp = g.row_ptrs.astype(np.int64)
+    owner = np.repeat(np.arange(g.V, dtype=np.int64), np.diff(rp))
+    out = np.bincount(owner[g.cols.astype(np.int64) > owner], minlength=g.V)
+    top = np.argsort(deg, kind="stable")[-64:]
+    wide = np.argsort(out, kind="stable")[::-1]
+    wide = np.concatenate([wide[:16], wide[16:20000:500]])
+    rand = np.random.default_rng(seed).choice(g.V, size=500, replace=False)
+    return np.unique(np.concatenate([top, wide, rand])).astype(np.uint32), top, wide
+
+
+def test_c2_bench_operators_on_hub_roots(vs, orc, rmat22):
+    """The operators the bench times, with its default knobs (4-cycle wedge
+    aggregation with heavy-root groups, fused 4-clique tail, diamond set reuse), and
+    their alternative kernels, on R-MAT 22 roots that include the hubs: exact
+    against the oracle.  4-cycles are attributed to their largest vertex by the
+    aggregation, 4-cliques to their smallest by every clique kernel."""
+    g, plans = rmat22
+    src, top, wide = hub_sample(g)
+    kc4, p1, p2 = plans
+    want = [orc.cliques_by_smallest(4, g, src), orc.c4_by_largest_wedges(g, src), orc.count(p2, g, src)]
+    assert min(want) > 0
+    with vs.Engine(g.V, plans) as e:
+        e.transfer_view(g, src)
+        e.match()
+        assert e.counts() == want
+        # the alternatives the knobs select, one at a time
+        for name, value, plan in (("tail_merge", 1, 0), ("fuse_tail", 0, 0), ("lane_slice", 0, 0), ("c4_heavy", 0, 1),
+                                  ("c4_heavy", 1 << 40, 1), ("set_reuse", 0, 2)):
+            e.set_option(name, value, plan=plan)
+            e.reset_counts()
+            e.match()
+            assert e.counts() == want, (name, value)
+            e.set_option(name, {"tail_merge": 0, "fuse_tail": 1, "lane_slice": 16, "c4_heavy": 1 << 16, "set_reuse": 1}[name], plan=plan)
 
 
 @pytest.mark.skipif(os.environ.get("VSGM_LARGE") != "1", reason="65M-vertex graph: set VSGM_LARGE=1")
