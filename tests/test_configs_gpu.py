@@ -80,8 +80,8 @@ def hub_sample(g, seed=21):
 
 def test_c2_bench_operators_on_hub_roots(vs, orc, rmat22):
     """The operators the bench times, with its default knobs (4-cycle wedge
-    aggregation with heavy-root groups, fused 4-clique tail, diamond set reuse), and
-    their alternative kernels, on R-MAT 22 roots that include the hubs: exact
+    aggregation with heavy-root groups, bitmap 4-clique operator, diamond set reuse),
+    and their alternative kernels (the plan's fused 4-clique tail and its variants), on R-MAT 22 roots that include the hubs: exact
     against the oracle.  4-cycles are attributed to their largest vertex by the
     aggregation, 4-cliques to their smallest by every clique kernel."""
     g, plans = rmat22
@@ -89,18 +89,15 @@ def test_c2_bench_operators_on_hub_roots(vs, orc, rmat22):
     kc4, p1, p2 = plans
     want = [orc.cliques_by_smallest(4, g, src), orc.c4_by_largest_wedges(g, src), orc.count(p2, g, src)]
     assert min(want) > 0
-    with vs.Engine(g.V, plans) as e:
-        e.transfer_view(g, src)
-        e.match()
-        assert e.counts() == want
-        # the alternatives the knobs select, one at a time
-        for name, value, plan in (("tail_merge", 1, 0), ("fuse_tail", 0, 0), ("lane_slice", 0, 0), ("c4_heavy", 0, 1),
-                                  ("c4_heavy", 1 << 40, 1), ("set_reuse", 0, 2)):
-            e.set_option(name, value, plan=plan)
-            e.reset_counts()
+    # the defaults, then the alternatives the knobs select
+    for knobs in ({}, {"clique_bits": 0}, {"clique_bits": 0, "tail_merge": 1}, {"clique_bits": 0, "fuse_tail": 0},
+                  {"clique_bits": 0, "lane_slice": 0}, {"c4_heavy": 0}, {"c4_heavy": 1 << 40}, {"set_reuse": 0}):
+        with vs.Engine(g.V, plans) as e:
+            for name, value in knobs.items():
+                e.set_option(name, value)
+            e.transfer_view(g, src)
             e.match()
-            assert e.counts() == want, (name, value)
-            e.set_option(name, {"tail_merge": 0, "fuse_tail": 1, "lane_slice": 16, "c4_heavy": 1 << 16, "set_reuse": 1}[name], plan=plan)
+            assert e.counts() == want, knobs
 
 
 @pytest.mark.skipif(os.environ.get("VSGM_LARGE") != "1", reason="65M-vertex graph: set VSGM_LARGE=1")

@@ -82,6 +82,7 @@ def test_stats_match_oracle_paths(vs, orc, graphs):
         total, paths = orc.op_paths(p, g)
         with vs.Engine(g.V, [p]) as e:
             e.set_option("c4_aggregate", 0)  # the op sequence itself
+            e.set_option("clique_bits", 0)
             e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
             e.match()
             assert e.counts() == [total]
@@ -186,6 +187,7 @@ def test_fused_tail_on_and_off(vs, orc, graphs, fuse):
              vs.plan_pattern(8), vs.plan_pattern(16), vs.plan_pattern(18)]
     with vs.Engine(g.V, plans) as e:
         e.set_option("fuse_tail", fuse)
+        e.set_option("clique_bits", 0)  # the cliques through the plan's fused tail too
         e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
         e.match()
         assert e.counts() == [orc.count(p, g) for p in plans]
@@ -219,6 +221,7 @@ def test_fused_tail_large_staged_sets(vs, orc, graphs):
         for cap in (1536, 16, 0):
             with vs.Engine(g.V, plans) as e:
                 e.set_option("stage_cap", cap)
+                e.set_option("clique_bits", 0)
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
                 e.match()
                 assert e.counts() == want, cap
@@ -235,6 +238,7 @@ def test_tail_merge_matches_oracle(vs, orc, graphs, gname):
     for ls in (0, 16):
         with vs.Engine(g.V, plans) as e:
             e.set_option("tail_merge", 1)
+            e.set_option("clique_bits", 0)
             e.set_option("lane_slice", ls)
             e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
             e.match()
@@ -303,6 +307,7 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
     want = [orc.count(p, g) for p in plans]
     with vs.Engine(g.V, plans) as e:
         e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+        e.set_option("clique_bits", 0)  # the 4-clique through the plan's intersections
         for ratio in (0, 1, 2, 64):
             for lane in (0, 1):
                 e.set_option("merge_ratio", ratio)
@@ -318,6 +323,7 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
                 e.match()
                 assert e.counts() == want, (walk, ls)
         e.set_option("lane_slice", 16)
+        e.set_option("clique_bits", 1)
         report = autotune(e, len(plans), stride=4)
         assert [r["plan"] for r in report] == list(range(len(plans)))
         e.match()
@@ -369,3 +375,63 @@ def test_set_reuse_pairs(vs, orc, graphs, reuse):
         e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
         e.match()
         assert e.counts() == [orc.count(p, g) for p in plans]
+
+
+def _star_of_cliques(vs, sizes=(20, 150, 600, 2000), chords=3, seed=8):
+    """Disjoint hubs, hub h joined to its leaves, the leaves on a ring with random
+    chords, ids kept as built (each hub below its leaves): the hubs' out-degrees are
+    the sizes, one per tier of the clique operator (<= 32, <= 256, <= 1024, wider)."""
+    rng = np.random.default_rng(seed)
+    edges, base = set(), 0
+    for n in sizes:
+        h = base
+        leaves = list(range(base + 1, base + n + 1))
+        edges |= {(h, x) for x in leaves}
+        edges |= {(leaves[i], leaves[(i + 1) % n]) for i in range(n)}
+        for a, b in rng.integers(0, n, size=(chords * n, 2)):
+            if a != b:
+                edges.add((leaves[min(a, b)], leaves[max(a, b)]))
+        base += n + 1
+    rows = [[] for _ in range(base)]
+    for a, b in edges:
+        rows[a].append(b)
+        rows[b].append(a)
+    rp = np.zeros(base + 1, np.uint64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    return vs.Graph(rp, np.array([x for r in rows for x in sorted(set(r))], dtype=np.uint32))
+
+
+def test_clique_bits_every_tier(vs, orc, graphs):
+    """The bitmap clique operator (each root's out-neighbourhood as bit rows) in all
+    of its tiers and its fallback to the plan, per root and in total, against the
+    rooted clique oracle; dense rows on complete graphs against closed forms."""
+    from math import comb
+    star = _star_of_cliques(vs)
+    kc = [vs.plan_clique(3), vs.plan_clique(4)]
+    for g in (star, graphs["rmat8"], graphs["chunglu"], vs.degree_relabel(graphs["rmat8"])[0], complete_graph(vs, 300)):
+        want = [orc.cliques_by_smallest(3, g), orc.cliques_by_smallest(4, g)]
+        for bits in (1, 0):
+            with vs.Engine(g.V, kc) as e:
+                e.set_option("clique_bits", bits)
+                e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+                e.match()
+                assert e.counts() == want, (bits, g.V)
+                # root subsets: the per-root attribution (smallest vertex)
+                for src in (np.arange(0, g.V, 3, dtype=np.uint32), np.array([0, 21, 172, 773], np.uint32) % g.V):
+                    src = np.unique(src)
+                    e.reset_counts()
+                    e.transfer_view(g, src)
+                    e.match()
+                    assert e.counts() == [orc.cliques_by_smallest(3, g, src), orc.cliques_by_smallest(4, g, src)], (bits, g.V)
+    # K_1100: every row full, roots 0..74 wider than the block tier
+    k = complete_graph(vs, 1100)
+    with vs.Engine(k.V, kc) as e:
+        e.transfer_view(k, np.arange(k.V, dtype=np.uint32))
+        e.match()
+        assert e.counts() == [comb(1100, 3), comb(1100, 4)]
+        # out-degree 1099 - u: 1025 / 1024 / 257 / 256 / 33 / 32 / 3 / 2 at the tier edges
+        for u in (0, 74, 75, 842, 843, 1066, 1067, 1096, 1097, 1099):
+            e.reset_counts()
+            e.transfer_view(k, np.array([u], np.uint32))
+            e.match()
+            assert e.counts() == [comb(1099 - u, 2), comb(1099 - u, 3)], u

@@ -1,6 +1,6 @@
 """Autotuner for the engine's per-plan knobs (intersection variant and tail fusion).
 
-For every plan it times each candidate setting of (c4_aggregate, fuse_tail,
+For every plan it times each candidate setting of (clique_bits, c4_aggregate, fuse_tail,
 merge_ratio, lane_merge, stage_cap, walk_ratio) on a strided sample of the view's roots (engine option root_stride)
 and keeps the fastest; the choice is written back as per-plan options.  Counts
 never depend on these knobs, so tuning on a sample is safe; the sample only has
@@ -10,6 +10,7 @@ import itertools
 import time
 
 CANDIDATES = {
+    "clique_bits": (1, 0),
     "c4_aggregate": (1, 0),
     "fuse_tail": (1, 0),
     "merge_ratio": (0, 4, 16),
@@ -27,6 +28,8 @@ def _settings(space):
             continue  # the stage and the walk only matter for the fused tail
         if cfg.get("lane_merge") and not cfg["merge_ratio"]:
             continue  # no merge, nothing to partition
+        if cfg.get("clique_bits") and not cfg.get("c4_aggregate", 1):
+            continue  # a plan is a clique or a 4-cycle, never both: one of the two settings suffices
         if cfg.get("c4_aggregate") and (cfg["fuse_tail"] != space["fuse_tail"][0] or cfg["merge_ratio"] != space["merge_ratio"][0]
                                         or cfg.get("lane_merge") or cfg["stage_cap"] != space["stage_cap"][0]
                                         or cfg.get("walk_ratio", 0) != space.get("walk_ratio", (0,))[0]):

@@ -26,6 +26,7 @@
 #include <string>
 #include <vector>
 
+#include "clique.cuh"
 #include "dfs.cuh"
 #include "kernels.cuh"
 #include "vsgm.h"
@@ -125,6 +126,7 @@ struct vsgm_engine {
     uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
     uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
     bool tail_merge = false;           // fused tail: heavy children by a merge-path split over the lanes
+    bool clique_bits = true;           // 3- and 4-clique plans: bitmap operator on the roots' out-neighbourhoods
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -774,6 +776,89 @@ struct vsgm_engine {
     st->op_paths[last] += n;
   }
 
+  // k when the plan counts k-cliques at their smallest vertex: a complete pattern
+  // whose LARGER_THAN / LESS_THAN conditions order every pair of vertices (their
+  // transitive closure is a strict total order) with the root first; else 0
+  static int clique_order(const vsgm_plan& p) {
+    const int n = (int)p.n_vertices;
+    if (n < 3 || n > VSGM_MAX_QV || p.n_edges != (uint32_t)(n * (n - 1) / 2)) return 0;
+    bool less[VSGM_MAX_QV][VSGM_MAX_QV] = {};  // less[a][b]: a < b
+    auto take = [&](int u, const vsgm_conds& c) {
+      for (int k = 0; k < c.count; k++) {
+        if (c.op[k] == VSGM_LARGER_THAN) less[c.v[k]][u] = true;
+        if (c.op[k] == VSGM_LESS_THAN) less[u][c.v[k]] = true;
+      }
+    };
+    for (int u = 0; u < n; u++) {
+      take(u, p.compute_cond[u]);
+      take(u, p.materialize_cond[u]);
+      take(u, p.filter_cond[u]);
+    }
+    for (int k = 0; k < n; k++)
+      for (int a = 0; a < n; a++)
+        for (int b = 0; b < n; b++) less[a][b] |= less[a][k] && less[k][b];
+    const int root = p.op_vertex[0];
+    for (int a = 0; a < n; a++) {
+      if (less[a][a]) return 0;
+      for (int b = 0; b < n; b++)
+        if (a != b && !(less[a][b] || less[b][a])) return 0;
+      if (a != root && !less[root][a]) return 0;
+    }
+    return n;
+  }
+
+  // k-cliques (k = 3, 4) at the given roots by the bitmap operator (clique.cuh);
+  // roots whose out-neighbourhood is wider than its block tier run the plan.
+  void clique_bits(const uint32_t* roots, uint64_t n, int K) {
+    const int last = (int)plan->n_ops - 1;
+    const uint32_t* up = upper_offsets();
+    Mark m(arena);
+    begin_op();
+    CliqueTiers t;
+    for (int k = 0; k < 4; k++) t.root[k] = arena.take_n<uint32_t>(std::max<uint64_t>(n, 1), "clique tier roots");
+    t.count = arena.take_n<unsigned long long>(6, "clique tier counters");  // 4 tiers + 2 queue heads
+    CK(cudaMemsetAsync(t.count, 0, 6 * sizeof(unsigned long long), stream));
+    k_clique_split<<<grid_threads(n), 256, 0, stream>>>(d_rp, up, roots, n, (uint32_t)(K - 1), t);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_pinned, t.count, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    const uint64_t nt[4] = {h_pinned[0], h_pinned[1], h_pinned[2], h_pinned[3]};
+    unsigned long long* bytes = profiling ? d_bytes : nullptr;
+    uint64_t launches = 1;
+    if (nt[2]) {
+      if (K == 3)
+        k_clique_large<3><<<(unsigned)sms, kCliqueLargeWarps * kWarp, kCliqueLargeSmem, stream>>>(d_rp, d_ci, up, t.root[2], nt[2], t.count + 4, d_total, bytes);
+      else
+        k_clique_large<4><<<(unsigned)sms, kCliqueLargeWarps * kWarp, kCliqueLargeSmem, stream>>>(d_rp, d_ci, up, t.root[2], nt[2], t.count + 4, d_total, bytes);
+      launches++;
+    }
+    if (nt[1]) {
+      if (K == 3)
+        k_clique_mid<3><<<(unsigned)sms * 2, kCliqueMidWarps * kWarp, kCliqueMidSmem, stream>>>(d_rp, d_ci, up, t.root[1], nt[1], t.count + 5, d_total, bytes);
+      else
+        k_clique_mid<4><<<(unsigned)sms * 2, kCliqueMidWarps * kWarp, kCliqueMidSmem, stream>>>(d_rp, d_ci, up, t.root[1], nt[1], t.count + 5, d_total, bytes);
+      launches++;
+    }
+    if (nt[0]) {
+      if (K == 3)
+        k_clique_small<3><<<grid_warps(nt[0]), 256, 0, stream>>>(d_rp, d_ci, up, t.root[0], nt[0], d_total, bytes);
+      else
+        k_clique_small<4><<<grid_warps(nt[0]), 256, 0, stream>>>(d_rp, d_ci, up, t.root[0], nt[0], d_total, bytes);
+      launches++;
+    }
+    CK(cudaGetLastError());
+    end_op(last, launches);
+    st->op_paths[last] += n;
+    if (nt[3]) {
+      // the widest out-neighbourhoods: the level-wise plan on those roots
+      Frame f;
+      std::memset(&f, 0, sizeof(f));
+      f.P = nt[3];
+      f.col[plan->op_vertex[0]] = t.root[3];
+      process(1, f);
+    }
+  }
+
   // the DFS fused tail (DfsFused): the level-wise engine's fusable() rule
   static void dfs_fuse(const vsgm_plan& p, DfsPlan* d) {
     if (p.n_ops < 3) return;
@@ -1062,8 +1147,11 @@ struct vsgm_engine {
     }
     st->op_paths[0] += f.P;
     st->op_outputs[0] += f.P;
+    const int K = cur.clique_bits ? clique_order(*plan) : 0;
     if (cur.c4_aggregate && is_four_cycle(*plan)) {
       c4_aggregate(f.col[plan->op_vertex[0]], f.P);
+    } else if (K == 3 || K == 4) {
+      clique_bits(f.col[plan->op_vertex[0]], f.P, K);
     } else {
       process(1, f);
     }
@@ -1125,6 +1213,11 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     CK(cudaSetDevice(device));
     CK(cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    // the clique operator's tiers keep their rows in more than 48 KB of shared memory
+    CK(cudaFuncSetAttribute(k_clique_mid<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueMidSmem));
+    CK(cudaFuncSetAttribute(k_clique_mid<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueMidSmem));
+    CK(cudaFuncSetAttribute(k_clique_large<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueLargeSmem));
+    CK(cudaFuncSetAttribute(k_clique_large<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueLargeSmem));
     CK(cudaEventCreate(&e->ev0));
     CK(cudaEventCreate(&e->ev1));
     CK(cudaEventCreate(&e->ev_h0));
@@ -1379,6 +1472,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   }
   if (n == "c4_aggregate") {
     for (int k = lo; k < hi; k++) e->knobs[k].c4_aggregate = value != 0;
+    return VSGM_OK;
+  }
+  if (n == "clique_bits") {
+    for (int k = lo; k < hi; k++) e->knobs[k].clique_bits = value != 0;
     return VSGM_OK;
   }
   if (n == "tail_merge") {
