@@ -80,8 +80,9 @@ def hub_sample(g, seed=21):
 
 def test_c2_bench_operators_on_hub_roots(vs, orc, rmat22):
     """The operators the bench times, with its default knobs (4-cycle wedge
-    aggregation with heavy-root groups, bitmap 4-clique operator, diamond set reuse),
-    and their alternative kernels (the plan's fused 4-clique tail and its variants), on R-MAT 22 roots that include the hubs: exact
+    aggregation with heavy-root groups, bitmap 4-clique operator, diamond from per-edge
+    triangle counts), and their alternative kernels (the plan's fused 4-clique tail
+    and its variants, the diamond's set reuse and plain intersections), on R-MAT 22 roots that include the hubs: exact
     against the oracle.  4-cycles are attributed to their largest vertex by the
     aggregation, 4-cliques to their smallest by every clique kernel."""
     g, plans = rmat22
@@ -91,7 +92,8 @@ def test_c2_bench_operators_on_hub_roots(vs, orc, rmat22):
     assert min(want) > 0
     # the defaults, then the alternatives the knobs select
     for knobs in ({}, {"clique_bits": 0}, {"clique_bits": 0, "tail_merge": 1}, {"clique_bits": 0, "fuse_tail": 0},
-                  {"clique_bits": 0, "lane_slice": 0}, {"c4_heavy": 0}, {"c4_heavy": 1 << 40}, {"set_reuse": 0}):
+                  {"clique_bits": 0, "lane_slice": 0}, {"c4_heavy": 0}, {"c4_heavy": 1 << 40}, {"edge_triangles": 0},
+                  {"edge_triangles": 0, "set_reuse": 0}):
         with vs.Engine(g.V, plans) as e:
             for name, value in knobs.items():
                 e.set_option(name, value)

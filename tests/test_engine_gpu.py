@@ -372,6 +372,7 @@ def test_set_reuse_pairs(vs, orc, graphs, reuse):
     plans = [vs.plan_pattern(2)] + [p for _, p in all_plans(vs) if _.startswith("km")]
     with vs.Engine(g.V, plans) as e:
         e.set_option("set_reuse", reuse)
+        e.set_option("edge_triangles", 0)  # the diamond through the plan's ops
         e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
         e.match()
         assert e.counts() == [orc.count(p, g) for p in plans]
@@ -435,3 +436,35 @@ def test_clique_bits_every_tier(vs, orc, graphs):
             e.transfer_view(k, np.array([u], np.uint32))
             e.match()
             assert e.counts() == [comb(1099 - u, 2), comb(1099 - u, 3)], u
+
+
+def test_diamond_from_edge_triangles(vs, orc, graphs):
+    """The diamond (-p 2) from per-edge triangle counts: per root (any source subset,
+    so the triangles whose smallest vertex is a lower neighbour of a source count
+    too), on views built by halo, in every tier of the triangle kernels and with the
+    fallback to the plan when an out-neighbourhood is wider than the block tier."""
+    p = vs.plan_pattern(2)
+    star = _star_of_cliques(vs, sizes=(20, 150, 2000, 17000), chords=1)
+    for g in (star, graphs["rmat8"], graphs["chunglu"], vs.degree_relabel(graphs["rmat8"])[0], complete_graph(vs, 60)):
+        rng = np.random.default_rng(g.V)
+        subsets = [np.arange(g.V, dtype=np.uint32), np.sort(rng.choice(g.V, size=max(1, g.V // 5), replace=False)).astype(np.uint32),
+                   np.array([0, 21, 172, 2173], np.uint32) % g.V]
+        for src in subsets:
+            src = np.unique(src)
+            want = orc.count(p, g, src)
+            for tri in (1, 0):
+                with vs.Engine(g.V, [p]) as e:
+                    e.set_option("edge_triangles", tri)
+                    e.transfer_view(g, src)
+                    e.match()
+                    assert e.counts() == [want], (tri, g.V, len(src))
+    # views built by halo around interleaved bins (rows beyond the halo are empty)
+    g = graphs["chunglu"]
+    with vs.Engine(g.V, [p]) as e:
+        e.upload_graph(g)
+        for b in range(3):
+            src = np.arange(b, g.V, 3, dtype=np.uint32)
+            e.reset_counts()
+            e.materialize_view(src, p.hop)
+            e.match()
+            assert e.counts() == [orc.count(p, g, src)], b

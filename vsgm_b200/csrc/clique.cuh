@@ -46,10 +46,11 @@ struct CliqueTiers {
 };
 
 // Split roots by out-degree d = |N(v) above v| (up[v] = offset of the first
-// neighbour above v); roots with d < min_d hold no clique and are dropped.
+// neighbour above v) into d <= lim0 / lim1 / lim2 / wider; roots with d < min_d
+// are dropped (they hold no clique, or no triangle).
 // Warp-aggregated appends: one atomic per tier per warp step.
 __global__ void k_clique_split(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ up, const uint32_t* __restrict__ roots, uint64_t n,
-                               uint32_t min_d, CliqueTiers t) {
+                               uint32_t min_d, uint32_t lim0, uint32_t lim1, uint32_t lim2, CliqueTiers t) {
   const unsigned lane = lane_id();
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
@@ -60,7 +61,7 @@ __global__ void k_clique_split(const uint64_t* __restrict__ rp, const uint32_t* 
     if (i < n) {
       v = __ldg(roots + i);
       const uint64_t d = __ldg(rp + v + 1) - __ldg(rp + v) - __ldg(up + v);
-      if (d >= min_d) tier = d <= kCliqueSmall ? 0 : d <= kCliqueMid ? 1 : d <= kCliqueLarge ? 2 : 3;
+      if (d >= min_d) tier = d <= lim0 ? 0 : d <= lim1 ? 1 : d <= lim2 ? 2 : 3;
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -74,13 +75,16 @@ __global__ void k_clique_split(const uint64_t* __restrict__ rp, const uint32_t* 
   }
 }
 
-// Row i of O's induced adjacency: bit j (j > i) of row[] set iff O[j] is in N(O[i]).
-// Only N(O[i]) above O[i] can hold such O[j].  Walks that part (coalesced, up to
-// O's largest value) probing O in shared memory, unless it is much longer than the
-// rest of O, which is then probed in N(O[i]) instead.  Returns the algorithmic bytes
-// of the row (row offsets, and the shorter of the two lists).
-__device__ __forceinline__ uint32_t clique_build_row(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
-                                                     const uint32_t* O, uint32_t d, uint32_t i, uint32_t* row) {
+// Visits the pairs (i, j), j > i, with O[j] a neighbour of O[i]: on_match(j, pos)
+// with pos the position of O[j] in the adjacency array (inside O[i]'s row).  Only
+// N(O[i]) above O[i] can hold such O[j].  Walks that part (coalesced, up to O's
+// largest value) probing O in shared memory, unless it is much longer than the
+// rest of O, which is then probed in N(O[i]) instead.  Lanes call on_match
+// independently.  Returns the algorithmic bytes of the row (row offsets, and the
+// shorter of the two lists).
+template <typename OnMatch>
+__device__ __forceinline__ uint32_t out_row_matches(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
+                                                    const uint32_t* O, uint32_t d, uint32_t i, OnMatch&& on_match) {
   const unsigned lane = lane_id();
   const uint32_t rest = d - i - 1;
   if (rest == 0) return 0;
@@ -93,7 +97,7 @@ __device__ __forceinline__ uint32_t clique_build_row(const uint64_t* __restrict_
     for (uint32_t j = i + 1 + lane; j < d; j += kWarp) {
       const uint32_t x = O[j];
       const uint64_t q = lower_bound(ci, s, z, x);
-      if (q < z && __ldg(ci + q) == x) atomicOr(row + (j >> 5), 1u << (j & 31));
+      if (q < z && __ldg(ci + q) == x) on_match(j, q);
     }
     return 16 + 4 * rest;
   }
@@ -106,12 +110,18 @@ __device__ __forceinline__ uint32_t clique_build_row(const uint64_t* __restrict_
     if (x <= omax) {
       const uint32_t j = smem_lower_bound(O, lo, d, x);
       lo = j;
-      if (j < d && O[j] == x) atomicOr(row + (j >> 5), 1u << (j & 31));
+      if (j < d && O[j] == x) on_match(j, k);
     }
     walked += kWarp;
     if (__any_sync(kFull, x >= omax)) break;
   }
   return 16 + 4 * (uint32_t)(walked < len ? walked : len);
+}
+
+// Row i of O's induced adjacency: bit j (j > i) of row[] set iff O[j] is in N(O[i]).
+__device__ __forceinline__ uint32_t clique_build_row(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
+                                                     const uint32_t* O, uint32_t d, uint32_t i, uint32_t* row) {
+  return out_row_matches(rp, ci, up, O, d, i, [&](uint32_t j, uint64_t) { atomicOr(row + (j >> 5), 1u << (j & 31)); });
 }
 
 // sum over the set bits j of row i of popc(row_i & row_j), rows of `stride` words
@@ -289,6 +299,164 @@ __global__ void __launch_bounds__(kCliqueLargeWarps * kWarp, 1)
     }
     if (t) atomicAdd(total, t);
     if (bytes && tb) atomicAdd(bytes, tb);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Triangles per edge, for the diamond plan (pm_pipeline -p 2: two triangles on a
+// shared edge, src/query/pattern.h).  t[k], for the adjacency slot k of an edge
+// (u, v) with u < v (k inside u's row), receives the number of triangles on that
+// edge that have their smallest vertex among the roots given: each triangle
+// a < b < c is found once, at root a, as the pair (i, j) of row i of O = N(a) above
+// a (b = O[i], c = O[j]).  The edge (b, c) gets +1 at its slot, found by the walk;
+// the edges (a, b) and (a, c) collect per-member counts in shared memory (row
+// count of b plus column count of c) and are added once per root.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kTriSmall = 32;    // warp per root, O and counts in static shared memory
+constexpr uint32_t kTriMid = 1024;    // warp per root, 8 KB of shared memory per warp
+constexpr uint32_t kTriLarge = 16384; // block per root, 128 KB of shared memory
+constexpr size_t kTriMidSmem = 8ull * 2 * kTriMid * sizeof(uint32_t);
+constexpr size_t kTriLargeSmem = 2ull * kTriLarge * sizeof(uint32_t);
+
+// the triangles of one root a whose O (d members) and counters cnt[d] (zeroed) are
+// in shared memory; warps take rows wid, wid + nwarps, ...  Counter updates are
+// shared-memory atomics because other warps add column counts concurrently.
+__device__ __forceinline__ uint32_t edge_tri_rows(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
+                                                  const uint32_t* O, uint32_t* cnt, uint32_t d, uint32_t wid, uint32_t nwarps, uint32_t* __restrict__ t) {
+  const unsigned lane = lane_id();
+  uint32_t b = 0;
+  for (uint32_t i = wid; i + 1 < d; i += nwarps) {
+    uint32_t c = 0;
+    b += out_row_matches(rp, ci, up, O, d, i, [&](uint32_t j, uint64_t pos) {
+      atomicAdd(t + pos, 1u);
+      atomicAdd(cnt + j, 1u);
+      c++;
+    });
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+    if (lane == 0 && c) atomicAdd(cnt + i, c);
+  }
+  return b;
+}
+
+// d <= DMAX: a warp per root (roots popped from *head)
+template <uint32_t DMAX>
+__global__ void __launch_bounds__(256) k_edge_tri_warp(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
+                                                       const uint32_t* __restrict__ roots, uint64_t n, unsigned long long* __restrict__ head,
+                                                       uint32_t* __restrict__ t, unsigned long long* __restrict__ bytes) {
+  extern __shared__ uint32_t smem[];
+  const unsigned lane = lane_id(), wid = threadIdx.x / kWarp;
+  uint32_t* O = smem + (size_t)wid * 2 * DMAX;
+  uint32_t* cnt = O + DMAX;
+  unsigned long long acc_bytes = 0;
+  while (true) {
+    unsigned long long r = 0;
+    if (lane == 0) r = atomicAdd(head, 1ull);
+    r = __shfl_sync(kFull, r, 0);
+    if (r >= n) break;
+    const uint32_t a = __ldg(roots + r);
+    const uint64_t base = __ldg(rp + a) + __ldg(up + a);
+    const uint32_t d = (uint32_t)(__ldg(rp + a + 1) - base);
+    for (uint32_t k = lane; k < d; k += kWarp) {
+      O[k] = __ldg(ci + base + k);
+      cnt[k] = 0;
+    }
+    __syncwarp();
+    const uint32_t b = edge_tri_rows(rp, ci, up, O, cnt, d, 0, 1, t);
+    __syncwarp();
+    for (uint32_t k = lane; k < d; k += kWarp)
+      if (cnt[k]) atomicAdd(t + base + k, cnt[k]);
+    if (bytes && lane == 0) acc_bytes += 16 + 4ull * d + b;
+    __syncwarp();
+  }
+  acc_bytes = warp_sum(acc_bytes);
+  if (bytes && lane == 0 && acc_bytes) atomicAdd(bytes, acc_bytes);
+}
+
+// d <= kTriLarge: a block per root
+__global__ void __launch_bounds__(512, 1) k_edge_tri_block(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
+                                                           const uint32_t* __restrict__ roots, uint64_t n, unsigned long long* __restrict__ head,
+                                                           uint32_t* __restrict__ t, unsigned long long* __restrict__ bytes) {
+  extern __shared__ uint32_t smem[];
+  __shared__ unsigned long long s_root;
+  const unsigned lane = lane_id(), wid = threadIdx.x / kWarp, nwarps = blockDim.x / kWarp;
+  uint32_t* O = smem;
+  uint32_t* cnt = O + kTriLarge;
+  unsigned long long acc_bytes = 0;
+  while (true) {
+    if (threadIdx.x == 0) s_root = atomicAdd(head, 1ull);
+    __syncthreads();
+    const unsigned long long r = s_root;
+    if (r >= n) break;
+    const uint32_t a = __ldg(roots + r);
+    const uint64_t base = __ldg(rp + a) + __ldg(up + a);
+    const uint32_t d = (uint32_t)(__ldg(rp + a + 1) - base);
+    for (uint32_t k = threadIdx.x; k < d; k += blockDim.x) {
+      O[k] = __ldg(ci + base + k);
+      cnt[k] = 0;
+    }
+    __syncthreads();
+    const uint32_t b = edge_tri_rows(rp, ci, up, O, cnt, d, wid, nwarps, t);
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < d; k += blockDim.x)
+      if (cnt[k]) atomicAdd(t + base + k, cnt[k]);
+    if (bytes && lane == 0) acc_bytes += b + (wid == 0 ? 16 + 4ull * d : 0);
+    __syncthreads();  // the next root overwrites O and the counters
+  }
+  acc_bytes = warp_sum(acc_bytes);
+  if (bytes && lane == 0 && acc_bytes) atomicAdd(bytes, acc_bytes);
+}
+
+// roots whose triangles can lie on an out-edge of a source s: s itself and its
+// neighbours below it (a triangle on (s, v), s < v, has its smallest vertex at s
+// or at a common neighbour below s)
+__global__ void k_tri_mark_roots(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
+                                 const uint32_t* __restrict__ src, uint64_t n, uint8_t* __restrict__ flags) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < n; i += warps) {
+    const uint32_t s = __ldg(src + i);
+    if (lane == 0) set_flag(flags, s);
+    const uint64_t a = __ldg(rp + s), z = a + __ldg(up + s);
+    for (uint64_t k = a + lane; k < z; k += kWarp) set_flag(flags, __ldg(ci + k));
+  }
+}
+
+__global__ void k_flags_to_list(const uint8_t* __restrict__ flags, uint64_t V, uint32_t* __restrict__ out, unsigned long long* __restrict__ count) {
+  const unsigned lane = lane_id();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < V; base += stride) {
+    const uint64_t v = base + lane;
+    const bool on = v < V && flags[v];
+    const unsigned m = __ballot_sync(kFull, on);
+    if (!m) continue;
+    unsigned long long at = 0;
+    if (lane == (unsigned)(__ffs(m) - 1)) at = atomicAdd(count, (unsigned long long)__popc(m));
+    at = __shfl_sync(kFull, at, __ffs(m) - 1);
+    if (on) out[at + __popc(m & ((1u << lane) - 1))] = (uint32_t)v;
+  }
+}
+
+// per source a: sum over its edges (a, b), b > a, of the pairs of the t(a, b)
+// common neighbours (mode 1: C(t, 2), the two wings ordered; mode 2: t (t - 1))
+__global__ void k_diamond_sum(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ up, const uint32_t* __restrict__ src, uint64_t n,
+                              const uint32_t* __restrict__ t, int mode, unsigned long long* __restrict__ total, unsigned long long* __restrict__ bytes) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  unsigned long long acc = 0, acc_bytes = 0;
+  for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < n; i += warps) {
+    const uint32_t s = __ldg(src + i);
+    const uint64_t z = __ldg(rp + s + 1), a = __ldg(rp + s) + __ldg(up + s);
+    for (uint64_t k = a + lane; k < z; k += kWarp) {
+      const unsigned long long c = __ldg(t + k);
+      acc += mode == 1 ? c * (c ? c - 1 : 0) / 2 : c * (c ? c - 1 : 0);
+    }
+    if (lane == 0) acc_bytes += 16 + 4 * (z - a);
+  }
+  acc = warp_sum(acc);
+  if (bytes) acc_bytes = warp_sum(acc_bytes);
+  if (lane == 0) {
+    if (acc) atomicAdd(total, acc);
+    if (bytes && acc_bytes) atomicAdd(bytes, acc_bytes);
   }
 }
 

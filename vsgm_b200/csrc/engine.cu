@@ -127,6 +127,7 @@ struct vsgm_engine {
     uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
     bool tail_merge = false;           // fused tail: heavy children by a merge-path split over the lanes
     bool clique_bits = true;           // 3- and 4-clique plans: bitmap operator on the roots' out-neighbourhoods
+    bool edge_triangles = true;        // diamond plans: pairs of per-edge triangle counts
   };
   std::vector<Knobs> knobs;
   Knobs cur;
@@ -818,7 +819,7 @@ struct vsgm_engine {
     for (int k = 0; k < 4; k++) t.root[k] = arena.take_n<uint32_t>(std::max<uint64_t>(n, 1), "clique tier roots");
     t.count = arena.take_n<unsigned long long>(6, "clique tier counters");  // 4 tiers + 2 queue heads
     CK(cudaMemsetAsync(t.count, 0, 6 * sizeof(unsigned long long), stream));
-    k_clique_split<<<grid_threads(n), 256, 0, stream>>>(d_rp, up, roots, n, (uint32_t)(K - 1), t);
+    k_clique_split<<<grid_threads(n), 256, 0, stream>>>(d_rp, up, roots, n, (uint32_t)(K - 1), kCliqueSmall, kCliqueMid, kCliqueLarge, t);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_pinned, t.count, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
@@ -857,6 +858,92 @@ struct vsgm_engine {
       f.col[plan->op_vertex[0]] = t.root[3];
       process(1, f);
     }
+  }
+
+  // Pair mode (1: C(t, 2), 2: t (t - 1)) when the plan is M(a) C(b) M(b) C(o) CC(w)
+  // with b > a the only condition on b, o and w both drawn from N(a) and N(b) with no
+  // conditions but "differs from a / b" (which a common neighbour always does), and
+  // o, w ordered or distinct: the diamond of pm_pipeline -p 2.  Its count at root a
+  // is the sum over edges (a, b), b > a, of the pairs of their t(a, b) common
+  // neighbours.  Else 0.
+  static int diamond_mode(const vsgm_plan& p) {
+    if (p.n_vertices != 4 || p.n_edges != 5 || p.n_ops != 5) return 0;
+    const int want[5] = {VSGM_MATERIALIZE, VSGM_COMPUTE, VSGM_MATERIALIZE, VSGM_COMPUTE, VSGM_COMPUTE_COUNT};
+    for (int i = 0; i < 5; i++)
+      if (p.op_type[i] != want[i]) return 0;
+    const int a = p.op_vertex[0], b = p.op_vertex[1], o = p.op_vertex[3], w = p.op_vertex[4];
+    if (p.op_vertex[2] != b || a == b || o == w || o == a || o == b || w == a || w == b) return 0;
+    if (p.backward[b].count != 1 || p.backward[b].v[0] != a) return 0;
+    if (p.compute_cond[b].count != 1 || p.compute_cond[b].op[0] != VSGM_LARGER_THAN || p.compute_cond[b].v[0] != a) return 0;
+    if (p.materialize_cond[b].count || p.materialize_cond[a].count) return 0;
+    for (int x : {o, w}) {
+      const vsgm_vgroup& B = p.backward[x];
+      if (B.count != 2 || !((B.v[0] == a && B.v[1] == b) || (B.v[0] == b && B.v[1] == a))) return 0;
+      const vsgm_conds& c = p.compute_cond[x];
+      for (int k = 0; k < c.count; k++)
+        if (c.op[k] != VSGM_NON_EQUAL || (c.v[k] != a && c.v[k] != b)) return 0;
+    }
+    if (p.computed_unmat[4].count != 1 || p.computed_unmat[4].v[0] != o) return 0;
+    const uint8_t rel = p.order[w][o];
+    return (rel == VSGM_LESS_THAN || rel == VSGM_LARGER_THAN) ? 1 : (rel == VSGM_NON_EQUAL ? 2 : 0);
+  }
+
+  // The diamond plan at the given roots from per-edge triangle counts (clique.cuh):
+  // the triangles with their smallest vertex among the roots or their neighbours
+  // below them are found once each and added to the slots of their three edges, then
+  // every root sums the pairs over its out-edges.  A view with an out-neighbourhood
+  // wider than the block tier runs the plan instead.
+  void diamond_edges(const uint32_t* roots, uint64_t n, int mode) {
+    const int last = (int)plan->n_ops - 1;
+    const uint32_t* up = upper_offsets();
+    Mark m(arena);
+    begin_op();
+    uint8_t* flags = (uint8_t*)arena.take_n<uint32_t>((V + 3) / 4 + 1, "triangle root flags");
+    uint32_t* R = arena.take_n<uint32_t>(std::max<uint64_t>(V, 1), "triangle roots");
+    CliqueTiers t;
+    for (int k = 0; k < 4; k++) t.root[k] = arena.take_n<uint32_t>(std::max<uint64_t>(V, 1), "triangle tier roots");
+    t.count = arena.take_n<unsigned long long>(8, "triangle counters");  // 4 tiers, 3 queue heads, the root count
+    CK(cudaMemsetAsync(flags, 0, sizeof(uint32_t) * ((V + 3) / 4 + 1), stream));
+    CK(cudaMemsetAsync(t.count, 0, 8 * sizeof(unsigned long long), stream));
+    k_tri_mark_roots<<<grid_warps(n), 256, 0, stream>>>(d_rp, d_ci, up, roots, n, flags);
+    k_flags_to_list<<<grid_threads(V), 256, 0, stream>>>(flags, V, R, t.count + 7);
+    CK(cudaGetLastError());
+    const uint64_t nR = read_u64((const uint64_t*)(t.count + 7));
+    k_clique_split<<<grid_threads(nR), 256, 0, stream>>>(d_rp, up, R, nR, 2u, kTriSmall, kTriMid, kTriLarge, t);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h_pinned, t.count, 4 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    const uint64_t nt[4] = {h_pinned[0], h_pinned[1], h_pinned[2], h_pinned[3]};
+    if (nt[3]) {
+      end_op(last, 3);
+      Frame f;
+      std::memset(&f, 0, sizeof(f));
+      f.P = n;
+      f.col[plan->op_vertex[0]] = const_cast<uint32_t*>(roots);
+      process(1, f);
+      return;
+    }
+    uint32_t* tri = arena.take_n<uint32_t>(std::max<uint64_t>(n_cols, 1), "per-edge triangle counts");
+    CK(cudaMemsetAsync(tri, 0, sizeof(uint32_t) * std::max<uint64_t>(n_cols, 1), stream));
+    unsigned long long* bytes = profiling ? d_bytes : nullptr;
+    uint64_t launches = 5;
+    if (nt[2]) {
+      k_edge_tri_block<<<(unsigned)sms, 512, kTriLargeSmem, stream>>>(d_rp, d_ci, up, t.root[2], nt[2], t.count + 4, tri, bytes);
+      launches++;
+    }
+    if (nt[1]) {
+      k_edge_tri_warp<kTriMid><<<(unsigned)sms * 3, 256, kTriMidSmem, stream>>>(d_rp, d_ci, up, t.root[1], nt[1], t.count + 5, tri, bytes);
+      launches++;
+    }
+    if (nt[0]) {
+      k_edge_tri_warp<kTriSmall><<<(unsigned)sms * 8, 256, 8 * 2 * kTriSmall * sizeof(uint32_t), stream>>>(d_rp, d_ci, up, t.root[0], nt[0], t.count + 6,
+                                                                                                       tri, bytes);
+      launches++;
+    }
+    k_diamond_sum<<<grid_warps(n), 256, 0, stream>>>(d_rp, up, roots, n, tri, mode, d_total, bytes);
+    CK(cudaGetLastError());
+    end_op(last, launches);
+    st->op_paths[last] += n;
   }
 
   // the DFS fused tail (DfsFused): the level-wise engine's fusable() rule
@@ -1152,6 +1239,8 @@ struct vsgm_engine {
       c4_aggregate(f.col[plan->op_vertex[0]], f.P);
     } else if (K == 3 || K == 4) {
       clique_bits(f.col[plan->op_vertex[0]], f.P, K);
+    } else if (const int dm = cur.edge_triangles ? diamond_mode(*plan) : 0) {
+      diamond_edges(f.col[plan->op_vertex[0]], f.P, dm);
     } else {
       process(1, f);
     }
@@ -1218,6 +1307,8 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     CK(cudaFuncSetAttribute(k_clique_mid<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueMidSmem));
     CK(cudaFuncSetAttribute(k_clique_large<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueLargeSmem));
     CK(cudaFuncSetAttribute(k_clique_large<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueLargeSmem));
+    CK(cudaFuncSetAttribute(k_edge_tri_warp<kTriMid>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTriMidSmem));
+    CK(cudaFuncSetAttribute(k_edge_tri_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTriLargeSmem));
     CK(cudaEventCreate(&e->ev0));
     CK(cudaEventCreate(&e->ev1));
     CK(cudaEventCreate(&e->ev_h0));
@@ -1472,6 +1563,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   }
   if (n == "c4_aggregate") {
     for (int k = lo; k < hi; k++) e->knobs[k].c4_aggregate = value != 0;
+    return VSGM_OK;
+  }
+  if (n == "edge_triangles") {
+    for (int k = lo; k < hi; k++) e->knobs[k].edge_triangles = value != 0;
     return VSGM_OK;
   }
   if (n == "clique_bits") {
