@@ -18,7 +18,8 @@ e2e     = the same through the C ABI from pinned host buffers: view upload +
           match + count read-back inside the timed region
 roofline: dominant kernel (COMPUTE_COUNT) algorithmic bytes / its device time
 cpu_baseline / --impl reference: the CPU restatement of the reference executor
-          (oracle/) on a time-boxed random sample of roots, all host cores;
+          (oracle/) on a time-boxed random sample of roots, all host cores (the
+          reference arm builds its graph and plans without the product library);
           cpu_baseline.view_stages: the reference's own .bin reader and view
           materialisation (compiled from its sources) beside ours, on host and device.
 """
@@ -182,14 +183,28 @@ def view_stage_times(vs, eng, g, threads):
     return out
 
 
+def bench_config(args, world):
+    """The config dict both arms print (the driver compares them)."""
+    return dict(WORKLOAD, scale=args.scale, l2="inputs larger than L2 (cols 0.5 GB)", parallelism=f"roots strided over {world} GPU(s)")
+
+
 def run_reference(args):
-    import torch.distributed as dist  # noqa: F401  (rank handling only)
+    """The reference arm: the CPU restatement of the reference executor (oracle/) on
+    all host cores, over the same graph (built by the oracle's restatement of the
+    generator) and the reference planner's own plans (its dump in tests/golden), on
+    a time-boxed random root sample per step.  Nothing of the product is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import vsgm_b200 as vs
-    vs.capi.lib()
-    g, plans = make_workload(vs, scale=args.scale, relabel=args.relabel, queries=args.query_flags)
+    import oracle
+    if args.relabel == "desc":
+        raise SystemExit("the reference arm restates ascending or no relabelling only")
+    t = time.time()
+    g = oracle.gen_rmat(args.scale, 16, 0.57, 0.19, 0.19, seed=2)
+    if args.relabel == "asc":
+        g = oracle.degree_relabel(g)
+    plans = [oracle.golden_plan(f.replace("-", "").replace(" ", "")) for f in args.query_flags]
+    log(f"reference arm: graph V={g.V} E={len(g.cols)} built in {time.time() - t:.1f}s from the oracle's generator; plans from the reference planner's dump")
     threads = os.cpu_count() or 1
     per_step = []
     for s in range(args.warmup + args.steps):
@@ -200,9 +215,10 @@ def run_reference(args):
     secs = float(np.mean([r[2] for r in per_step]))
     sample = (f"{per_step[-1][3]} random roots of {g.V} per step (time-boxed {args.ref_seconds}s, summed over the {len(plans)} queries); "
               f"matches/s = sampled matches / sampled seconds")
-    out = {"impl": "reference", "metric": "matches/s", "value": rate, "unit": "matches/s", "n_gpus": args.gpus, "steps": args.steps,
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    out = {"impl": "reference", "metric": "matches/s", "value": rate, "unit": "matches/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-           "dtype": "u32", "data": "synthetic", "config": WORKLOAD,
+           "dtype": "u32", "data": "synthetic", "config": bench_config(args, world),
            "cpu_baseline": {"value": rate, "unit": "matches/s", "cores": threads, "kind": "port", "sample": sample},
            "e2e": {"value": rate, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -360,8 +376,7 @@ def main():
     if rank == 0:
         out = {"metric": "matches/s", "value": value, "unit": "matches/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                "ms_per_step": step_ms, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
-               "data": "synthetic", "config": dict(WORKLOAD, scale=args.scale, l2="inputs larger than L2 (cols 0.5 GB)",
-                                                     parallelism=f"roots strided over {world} GPU(s)"),
+               "data": "synthetic", "config": bench_config(args, world),
                "counts": counts, "per_query": per_query, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                "gpu_launches": int(launches), "clocks": clocks}
         print(json.dumps(out), flush=True)

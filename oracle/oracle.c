@@ -38,6 +38,9 @@
  * 5. oracle_cliques_by_smallest: k-cliques whose smallest vertex is a source, by
  *    definition (ordered candidate sets) - the clique plans' per-root attribution,
  *    fast on hub roots; pinned to oracle_count root by root.
+ * 6. oracle_gen_rmat / oracle_degree_relabel: the benchmark's synthetic input
+ *    (R-MAT graph, ids ascending with degree), so that the timed CPU baseline
+ *    needs nothing from the product library.
  *
  * Parity: the reference's matching path cannot be built here (its moderngpu and
  * MPMCQueue submodules are not vendored and it needs a GPU), and the reference
@@ -459,3 +462,133 @@ uint64_t oracle_cliques_by_smallest(int k, uint64_t V, const uint64_t* rp, const
   }
   return total;
 }
+
+/* ------------------------------------------------------- workload (reference arm) */
+/* The benchmark's synthetic input, restated so that the timed CPU baseline builds
+ * it without the product library: the R-MAT generator (per edge i and level l one
+ * uniform double from a splitmix64 finaliser over a seed-salted counter i*64 + l;
+ * quadrant by a, a+b, a+b+c), then symmetrised with self loops and duplicates
+ * dropped and every row sorted - the layout the reference's preprocessing writes
+ * (src/preprocess/preprocess_graph.h:12-92).  tests/test_oracle.py checks it edge
+ * for edge against the library's generator. */
+static uint64_t wl_mix64(uint64_t seed, uint64_t i) {
+  uint64_t z = seed * 0x9E3779B97F4A7C15ull + i * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+static double wl_unit(uint64_t seed, uint64_t i) { return (double)(wl_mix64(seed, i) >> 11) * (1.0 / 9007199254740992.0); }
+
+static int cmp_u32(const void* a, const void* b) {
+  const uint32_t x = *(const uint32_t*)a, y = *(const uint32_t*)b;
+  return x < y ? -1 : x > y;
+}
+
+/* rows from (src, dst) edge lists: both directions, no loops, sorted, unique.
+ * *rp (V+1) and *ci are malloc'd here. */
+static void wl_csr(uint64_t V, const uint32_t* src, const uint32_t* dst, uint64_t m, int T, uint64_t** rp_out, uint32_t** ci_out) {
+  uint64_t* cnt = (uint64_t*)calloc(V + 1, sizeof(uint64_t));
+  for (uint64_t i = 0; i < m; i++)
+    if (src[i] != dst[i]) {
+      cnt[src[i] + 1]++;
+      cnt[dst[i] + 1]++;
+    }
+  for (uint64_t v = 0; v < V; v++) cnt[v + 1] += cnt[v];
+  uint32_t* tmp = (uint32_t*)malloc((cnt[V] ? cnt[V] : 1) * sizeof(uint32_t));
+  uint64_t* cur = (uint64_t*)malloc((V ? V : 1) * sizeof(uint64_t));
+  memcpy(cur, cnt, V * sizeof(uint64_t));
+  for (uint64_t i = 0; i < m; i++)
+    if (src[i] != dst[i]) {
+      tmp[cur[src[i]]++] = dst[i];
+      tmp[cur[dst[i]]++] = src[i];
+    }
+  uint64_t* kept = cur; /* reused: unique entries per row */
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
+  for (int64_t v = 0; v < (int64_t)V; v++) {
+    uint32_t* r = tmp + cnt[v];
+    const uint64_t n = cnt[v + 1] - cnt[v];
+    qsort(r, n, sizeof(uint32_t), cmp_u32);
+    uint64_t k = 0;
+    for (uint64_t j = 0; j < n; j++)
+      if (k == 0 || r[j] != r[k - 1]) r[k++] = r[j];
+    kept[v] = k;
+  }
+  uint64_t* rp = (uint64_t*)malloc((V + 1) * sizeof(uint64_t));
+  rp[0] = 0;
+  for (uint64_t v = 0; v < V; v++) rp[v + 1] = rp[v] + kept[v];
+  uint32_t* ci = (uint32_t*)malloc((rp[V] ? rp[V] : 1) * sizeof(uint32_t));
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
+  for (int64_t v = 0; v < (int64_t)V; v++) memcpy(ci + rp[v], tmp + cnt[v], kept[v] * sizeof(uint32_t));
+  free(tmp);
+  free(cur);
+  free(cnt);
+  *rp_out = rp;
+  *ci_out = ci;
+}
+
+void oracle_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed, int threads, uint64_t* V_out, uint64_t** rp,
+                     uint32_t** ci) {
+  const uint64_t V = 1ull << scale, m = (uint64_t)edge_factor << scale;
+  const int T = threads > 0 ? threads : omp_get_max_threads();
+  uint32_t* src = (uint32_t*)malloc(m * sizeof(uint32_t));
+  uint32_t* dst = (uint32_t*)malloc(m * sizeof(uint32_t));
+  const double ab = a + b, abc = a + b + c;
+#pragma omp parallel for num_threads(T) schedule(static)
+  for (int64_t i = 0; i < (int64_t)m; i++) {
+    uint64_t s = 0, d = 0;
+    for (int l = 0; l < scale; l++) {
+      const double r = wl_unit(seed, (uint64_t)i * 64 + l);
+      s <<= 1;
+      d <<= 1;
+      if (r < a) {
+      } else if (r < ab) {
+        d |= 1;
+      } else if (r < abc) {
+        s |= 1;
+      } else {
+        s |= 1;
+        d |= 1;
+      }
+    }
+    src[i] = (uint32_t)s;
+    dst[i] = (uint32_t)d;
+  }
+  wl_csr(V, src, dst, m, T, rp, ci);
+  free(src);
+  free(dst);
+  *V_out = V;
+}
+
+/* new id = rank of (degree, old id), ascending: a stable counting sort by degree;
+ * rows moved to their new ids, entries renamed and sorted.  Output malloc'd. */
+void oracle_degree_relabel(uint64_t V, const uint64_t* rp, const uint32_t* ci, int threads, uint64_t** rp_out, uint32_t** ci_out) {
+  const int T = threads > 0 ? threads : omp_get_max_threads();
+  const uint64_t dmax = max_degree(V, rp);
+  uint64_t* at = (uint64_t*)calloc(dmax + 2, sizeof(uint64_t));
+  for (uint64_t v = 0; v < V; v++) at[rp[v + 1] - rp[v] + 1]++;
+  for (uint64_t d = 0; d <= dmax; d++) at[d + 1] += at[d];
+  uint32_t* order = (uint32_t*)malloc((V ? V : 1) * sizeof(uint32_t));
+  uint32_t* nid = (uint32_t*)malloc((V ? V : 1) * sizeof(uint32_t));
+  for (uint64_t v = 0; v < V; v++) order[at[rp[v + 1] - rp[v]]++] = (uint32_t)v;
+  for (uint64_t r = 0; r < V; r++) nid[order[r]] = (uint32_t)r;
+  uint64_t* nrp = (uint64_t*)malloc((V + 1) * sizeof(uint64_t));
+  nrp[0] = 0;
+  for (uint64_t r = 0; r < V; r++) nrp[r + 1] = nrp[r] + (rp[order[r] + 1] - rp[order[r]]);
+  uint32_t* nci = (uint32_t*)malloc((nrp[V] ? nrp[V] : 1) * sizeof(uint32_t));
+#pragma omp parallel for num_threads(T) schedule(dynamic, 1024)
+  for (int64_t r = 0; r < (int64_t)V; r++) {
+    const uint32_t v = order[r];
+    uint32_t* dst = nci + nrp[r];
+    const uint64_t n = rp[v + 1] - rp[v];
+    for (uint64_t j = 0; j < n; j++) dst[j] = nid[ci[rp[v] + j]];
+    qsort(dst, n, sizeof(uint32_t), cmp_u32);
+  }
+  free(at);
+  free(order);
+  free(nid);
+  *rp_out = nrp;
+  *ci_out = nci;
+}
+
+void oracle_free(void* p) { free(p); }

@@ -112,3 +112,21 @@ def test_rooted_clique_oracle_equals_plan_oracle(vs, orc, g):
     for k in (3, 4, 5, 6, 7):
         for u in range(8):
             assert orc.cliques_by_smallest(k, kn, np.array([u], np.uint32)) == comb(7 - u, k - 1)
+
+
+def test_restated_workload_and_golden_plans(vs, orc):
+    """The reference arm's inputs, built without the product library, equal the
+    library's: the R-MAT graph and its degree relabelling edge for edge, and the
+    plans of the benchmark's queries table for table."""
+    for scale, ef, seed in ((10, 16, 2), (12, 8, 5)):
+        g = vs.gen_rmat(scale, ef, 0.57, 0.19, 0.19, seed=seed)
+        h = orc.gen_rmat(scale, ef, 0.57, 0.19, 0.19, seed=seed)
+        assert np.array_equal(g.row_ptrs, h.row_ptrs) and np.array_equal(g.cols, h.cols)
+        gr, _ = vs.degree_relabel(g, ascending=True)
+        hr = orc.degree_relabel(h)
+        assert np.array_equal(gr.row_ptrs, hr.row_ptrs) and np.array_equal(gr.cols, hr.cols)
+    import ctypes as C
+    for name, p in (("kc4", vs.plan_clique(4)), ("p1", vs.plan_pattern(1)), ("p2", vs.plan_pattern(2))):
+        q = orc.golden_plan(name)
+        assert bytes(q)[:C.sizeof(q)] == bytes(p)[:C.sizeof(p)], name
+        assert orc.count(q, hr) == orc.count(p, hr)
