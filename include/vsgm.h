@@ -133,7 +133,12 @@ int vsgm_bind_view_device(vsgm_engine* e, const uint64_t* d_row_ptrs, const uint
 
 /* Keep the whole graph resident on the engine's device (row_ptrs[V+1], cols)
  * so that views can be built there: replaces the host producers of
- * src/app/pattern_matching_pipeline.cu:117-150 (one LoadViewBin per bin). */
+ * src/app/pattern_matching_pipeline.cu:117-150 (one LoadViewBin per bin).  With the
+ * engine option "relabel" set, the graph (undirected: both directions stored) is
+ * relabelled on the device so that ids ascend with (degree, id) - the permutation
+ * of vsgm_degree_relabel - and the sources given to vsgm_graph_view /
+ * vsgm_materialize_view stay in the caller's ids; totals do not change, and
+ * vsgm_read_view then returns the relabelled rows. */
 int vsgm_upload_graph(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n_cols);
 
 /* ViewBin::Materialize (src/view/view_bin.h:66-142) on the device from the
@@ -226,6 +231,16 @@ const char* vsgm_mlp_error(vsgm_mlp* m);
 int vsgm_mlp_destroy(vsgm_mlp* m);
 
 /* Tuning knobs (no reference counterpart), for every plan or for one plan:
+ *   "clique_bits" (default 1): a 3- or 4-clique plan (complete pattern, every pair
+ *   of vertices ordered, the root first) counts at each root the cliques of its
+ *   out-neighbourhood from bit rows of that neighbourhood's adjacency in shared
+ *   memory; roots with more than 1024 neighbours above them run the plan;
+ *   "edge_triangles" (default 1): the diamond plan (-p 2) is counted from per-edge
+ *   triangle counts (each triangle found once, at its smallest vertex) as the sum
+ *   over the root's edges to larger neighbours of the pairs of common neighbours;
+ *   a view with a vertex of more than 16384 neighbours above it runs the plan;
+ *   "relabel" (engine-wide, default 0): vsgm_upload_graph orders the resident
+ *   graph's ids by degree on the device (see there);
  *   "fuse_tail" (default 1): a MATERIALIZE followed by the final COMPUTE_COUNT runs as
  *   one kernel that stages the parent's shared lists in shared memory instead of
  *   expanding the children;
@@ -246,7 +261,7 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   set is at most this long is handled by one lane, longer ones by the whole warp;
  *   "tail_merge" (default 0): in the fused tail a heavy child intersects its slice
  *   and its part of N(c) by a merge-path split over the warp's lanes instead of
- *   the walk / gallop (experimental: not yet timed);
+ *   the walk / gallop;
  *   "c4_heavy" (default 2^16): roots with at least this many wedges are counted by
  *   groups sharing the whole GPU with L2-resident counters (0: every root);
  *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT

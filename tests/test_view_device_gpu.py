@@ -126,3 +126,32 @@ def test_pm_pipeline_device_views(vs, orc, graphs, tmp_path):
                              capture_output=True, text=True, timeout=300)
         assert out.returncode == 0, out.stderr
         assert int(re.search(r"total count for query 0: (\d+)", out.stdout).group(1)) == want
+
+
+def test_device_relabel_equals_host(vs, orc, graphs):
+    """vsgm_upload_graph with the "relabel" option: the resident graph equals the host
+    relabelling (ids ascending with (degree, id)) entry for entry, totals do not
+    change, and a bin given in the caller's ids counts what the oracle counts on the
+    relabelled graph at the mapped sources (4-cycles by their largest vertex)."""
+    from conftest import complete_graph, empty_graph
+    kc4, p1, p2 = vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2)
+    for g in (graphs["rmat8"], graphs["chunglu"], vs.gen_rmat(12, 16, seed=3), empty_graph(vs, 9), complete_graph(vs, 12)):
+        h, new_of_old = vs.degree_relabel(g, ascending=True)
+        with vs.Engine(g.V, [kc4, p1, p2]) as e:
+            e.set_option("relabel", 1)
+            e.upload_graph(g)
+            e.graph_view(np.arange(g.V, dtype=np.uint32))
+            r = e.read_view()
+            assert np.array_equal(r.row_ptrs, h.row_ptrs) and np.array_equal(r.cols, h.cols)
+            e.match()
+            assert e.counts() == [orc.count(p, g) for p in (kc4, p1, p2)]
+            src = np.arange(0, g.V, 3, dtype=np.uint32)
+            mapped = np.sort(new_of_old[src]).astype(np.uint32)
+            e.reset_counts()
+            e.graph_view(src)
+            e.match()
+            assert e.counts() == [orc.count(kc4, h, mapped), orc.c4_by_largest(h, mapped), orc.count(p2, h, mapped)]
+            e.reset_counts()
+            e.materialize_view(src, 2)
+            e.match()
+            assert e.counts() == [orc.count(kc4, h, mapped), orc.c4_by_largest(h, mapped), orc.count(p2, h, mapped)]

@@ -29,6 +29,7 @@
 #include "clique.cuh"
 #include "dfs.cuh"
 #include "kernels.cuh"
+#include "relabel.cuh"
 #include "vsgm.h"
 
 using namespace vsgm::dev;
@@ -101,6 +102,8 @@ struct vsgm_engine {
   uint64_t* g_rp = nullptr;
   uint32_t* g_ci = nullptr;
   uint64_t g_cols = 0;
+  bool relabel = false;         // option "relabel": vsgm_upload_graph orders ids by degree on the device
+  uint32_t* g_new = nullptr;    // new id of every caller id of the resident graph (when relabelled)
   // per view: offset of each vertex's first larger neighbour (fused tails with a "> child" condition)
   uint32_t* d_up = nullptr;
   const uint64_t* up_of = nullptr;  // the row_ptrs d_up was computed for
@@ -215,6 +218,64 @@ struct vsgm_engine {
     else
       k_scan_apply<false><<<(unsigned)tiles, kScanThreads, 0, stream>>>(in, n, sums, out);
     CK(cudaGetLastError());
+  }
+
+  // Stable radix sort of n (key, value) pairs by the low `bits` bits of the keys,
+  // ping-ponging between (k0, v0) and (k1, v1); true when the result is in (k1, v1).
+  bool radix_sort(uint32_t* k0, uint32_t* v0, uint32_t* k1, uint32_t* v1, uint64_t n, int bits) {
+    if (n == 0) return false;
+    const uint64_t tiles = (n + kRadixTile - 1) / kRadixTile;
+    Mark m(arena);
+    uint32_t* hist = arena.take_n<uint32_t>(256 * tiles, "radix histogram");
+    uint64_t* off = arena.take_n<uint64_t>(256 * tiles + 1, "radix offsets");
+    bool in1 = false;
+    for (int shift = 0; shift < bits; shift += 8) {
+      const uint32_t* ks = in1 ? k1 : k0;
+      const uint32_t* vs = in1 ? v1 : v0;
+      k_radix_hist<<<(unsigned)tiles, kRadixThreads, 0, stream>>>(ks, n, shift, hist, tiles);
+      CK(cudaGetLastError());
+      scan(hist, true, 256 * tiles, off);
+      k_radix_scatter<<<(unsigned)tiles, kRadixThreads, 0, stream>>>(ks, vs, n, shift, off, tiles, in1 ? k0 : k1, in1 ? v0 : v1);
+      CK(cudaGetLastError());
+      in1 = !in1;
+    }
+    return in1;
+  }
+
+  // The resident graph from the caller's (t_rp, t_ci), relabelled so that ids ascend
+  // with degree (relabel.cuh), into g_rp / g_ci, with the caller-id map in g_new.
+  void relabel_into_resident(const uint64_t* t_rp, const uint32_t* t_ci, uint64_t E) {
+    auto bits_of = [](uint64_t x) {
+      int b = 0;
+      while (b < 64 && (x >> b)) b++;
+      return b;
+    };
+    Mark m(arena);
+    const uint64_t Vn = std::max<uint64_t>(V, 1);
+    uint32_t* dk0 = arena.take_n<uint32_t>(Vn, "relabel degree keys");
+    uint32_t* dv0 = arena.take_n<uint32_t>(Vn, "relabel ids");
+    uint32_t* dk1 = arena.take_n<uint32_t>(Vn, "relabel degree keys");
+    uint32_t* dv1 = arena.take_n<uint32_t>(Vn, "relabel ids");
+    uint64_t* len = arena.take_n<uint64_t>(Vn, "relabel row lengths");
+    unsigned long long* dmax = arena.take_n<unsigned long long>(1, "relabel max degree");
+    CK(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), stream));
+    k_degree_pairs<<<grid_threads(V), 256, 0, stream>>>(t_rp, V, dk0, dv0, dmax);
+    CK(cudaGetLastError());
+    const uint64_t dm = read_u64((const uint64_t*)dmax);
+    if (dm >= 0xffffffffull) throw std::invalid_argument("relabel: a degree does not fit 32 bits");
+    const uint32_t* order = radix_sort(dk0, dv0, dk1, dv1, V, bits_of(dm)) ? dv1 : dv0;
+    k_invert_order<<<grid_threads(V), 256, 0, stream>>>(t_rp, order, V, g_new, len);
+    CK(cudaGetLastError());
+    scan(len, false, V, g_rp);
+    const uint64_t En = std::max<uint64_t>(E, 1);
+    uint32_t* ek0 = arena.take_n<uint32_t>(En, "relabel edge keys");
+    uint32_t* ev0 = arena.take_n<uint32_t>(En, "relabel edge values");
+    uint32_t* ek1 = arena.take_n<uint32_t>(En, "relabel edge keys");
+    uint32_t* ev1 = arena.take_n<uint32_t>(En, "relabel edge values");
+    k_emit_edges<<<grid_warps(V), 256, 0, stream>>>(t_rp, t_ci, order, g_new, g_rp, V, ek0, ev0);
+    CK(cudaGetLastError());
+    const uint32_t* sorted = radix_sort(ek0, ev0, ek1, ev1, E, bits_of(V - 1)) ? ev1 : ev0;
+    if (E) CK(cudaMemcpyAsync(g_ci, sorted, sizeof(uint32_t) * E, cudaMemcpyDeviceToDevice, stream));
   }
 
   // largest b in (a, P] with unit * (off[b] - off[a]) + item * (b - a) <= budget;
@@ -1392,10 +1453,24 @@ int vsgm_upload_graph(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* 
     if (e->g_ci) CK(cudaFree(e->g_ci));
     e->g_rp = nullptr;
     e->g_ci = nullptr;
+    if (e->g_new) CK(cudaFree(e->g_new));
+    e->g_new = nullptr;
     CK(cudaMalloc(&e->g_rp, sizeof(uint64_t) * (e->V + 1)));
     CK(cudaMalloc(&e->g_ci, sizeof(uint32_t) * std::max<uint64_t>(n_cols, 1)));
-    CK(cudaMemcpyAsync(e->g_rp, row_ptrs, sizeof(uint64_t) * (e->V + 1), cudaMemcpyHostToDevice, e->stream));
-    if (n_cols) CK(cudaMemcpyAsync(e->g_ci, cols, sizeof(uint32_t) * n_cols, cudaMemcpyHostToDevice, e->stream));
+    if (e->relabel) {
+      // the caller's graph goes to the arena first, the relabelled one stays resident
+      CK(cudaMalloc(&e->g_new, sizeof(uint32_t) * std::max<uint64_t>(e->V, 1)));
+      Mark m(e->arena);
+      e->arena.top = 0;
+      uint64_t* t_rp = e->arena.take_n<uint64_t>(e->V + 1, "graph row offsets (caller ids)");
+      uint32_t* t_ci = e->arena.take_n<uint32_t>(std::max<uint64_t>(n_cols, 1), "graph adjacency (caller ids)");
+      CK(cudaMemcpyAsync(t_rp, row_ptrs, sizeof(uint64_t) * (e->V + 1), cudaMemcpyHostToDevice, e->stream));
+      if (n_cols) CK(cudaMemcpyAsync(t_ci, cols, sizeof(uint32_t) * n_cols, cudaMemcpyHostToDevice, e->stream));
+      e->relabel_into_resident(t_rp, t_ci, n_cols);
+    } else {
+      CK(cudaMemcpyAsync(e->g_rp, row_ptrs, sizeof(uint64_t) * (e->V + 1), cudaMemcpyHostToDevice, e->stream));
+      if (n_cols) CK(cudaMemcpyAsync(e->g_ci, cols, sizeof(uint32_t) * n_cols, cudaMemcpyHostToDevice, e->stream));
+    }
     CK(cudaStreamSynchronize(e->stream));
     e->g_cols = n_cols;
   });
@@ -1417,6 +1492,7 @@ int vsgm_materialize_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_so
       e->src_cap = n_sources;
     }
     if (n_sources) CK(cudaMemcpyAsync(e->own_src, sources, sizeof(uint32_t) * n_sources, cudaMemcpyHostToDevice, e->stream));
+    if (n_sources && e->g_new) k_map_ids<<<e->grid_threads(n_sources), 256, 0, e->stream>>>(e->own_src, n_sources, e->g_new);
     Mark m(e->arena);
     e->arena.top = 0;
     // membership flags: one byte per vertex, whole words so the flag update is a word atomic
@@ -1474,6 +1550,8 @@ int vsgm_graph_view(vsgm_engine* e, const uint32_t* sources, uint64_t n_sources)
       e->src_cap = n_sources;
     }
     if (n_sources) CK(cudaMemcpyAsync(e->own_src, sources, sizeof(uint32_t) * n_sources, cudaMemcpyHostToDevice, e->stream));
+    if (n_sources && e->g_new) k_map_ids<<<e->grid_threads(n_sources), 256, 0, e->stream>>>(e->own_src, n_sources, e->g_new);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(e->stream));
     e->d_rp = e->g_rp;
     e->d_ci = e->g_ci;
@@ -1611,6 +1689,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
     e->hybrid_steps = (uint64_t)value;
     return VSGM_OK;
   }
+  if (n == "relabel") {
+    e->relabel = value != 0;
+    return VSGM_OK;
+  }
   if (n == "root_stride") {
     if (value < 1) return engine_fail(e, VSGM_EINVAL, "root_stride must be >= 1");
     e->root_stride = (uint64_t)value;
@@ -1730,6 +1812,7 @@ int vsgm_destroy(vsgm_engine* e) {
   cudaFree(e->own_src);
   cudaFree(e->g_rp);
   cudaFree(e->g_ci);
+  cudaFree(e->g_new);
   cudaFree(e->d_up);
   for (auto& r : e->rviews) {
     cudaFree(r.rp);

@@ -14,8 +14,9 @@
 // Either way one consumer per GPU matches every plan and accumulates exact
 // counts.  Without a .vbmap file (the file does not exist) every vertex is a source
 // of one bin; any other failure to open it is an error.  With -rl 1 (default) the
-// graph and its bins are relabelled so that ids ascend with degree before any view
-// is built (inside the timed region): the plans' order conditions then cut every
+// graph is relabelled so that ids ascend with degree before any view is built
+// (inside the timed region; on the device with -gv 1 / 2, on the host with the bins
+// following their vertices with -gv 0): the plans' order conditions then cut every
 // adjacency window short, and exact totals do not depend on the labelling.  Prints
 // "total count for query i: N" and "finish total time, elapsed_time=Xms" like the
 // reference.
@@ -179,8 +180,10 @@ int main(int argc, char** argv) {
     return std::fprintf(stderr, "error: %s\n", vsgm_last_error()), 1;
   }
   double t0 = now_us();
-  if (a.rl) {
-    // ids ascending with degree; the bins follow their vertices
+  if (a.rl && a.gv == 0) {
+    // views built on the host: relabel the host graph (ids ascending with degree;
+    // the bins follow their vertices).  With -gv 1 / 2 every consumer relabels its
+    // resident copy on the device instead, and the bins stay in the file's ids.
     std::vector<uint32_t> new_of_old(V);
     uint64_t* rp2 = (uint64_t*)std::malloc(sizeof(uint64_t) * (V + 1));
     uint32_t* ci2 = (uint32_t*)std::malloc(sizeof(uint32_t) * std::max<uint64_t>(E, 1));
@@ -261,6 +264,13 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(nullptr));
         failed = 1;
         while (View* v = q.pop()) delete v;  // keep producers moving
+        return;
+      }
+      if (a.gv && a.rl && vsgm_set_option(e, "relabel", 1)) {
+        std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(e));
+        failed = 1;
+        while (View* v = q.pop()) delete v;
+        vsgm_destroy(e);
         return;
       }
       if (a.gv && vsgm_upload_graph(e, rp, ci, E)) {
