@@ -14,8 +14,9 @@ A step is one match of all three queries over the resident view.
 for profiling; the default is the workload above.)
 
 value   = sum of the exact counts / device time per step (inputs resident in HBM)
-e2e     = the same through the C ABI from pinned host buffers: view upload +
-          match + count read-back inside the timed region
+e2e     = the same through the C ABI from pinned host buffers: the graph in the
+          generator's ids uploaded, relabelled by degree on the device, matched,
+          counts read back - all inside the timed region
 roofline: dominant kernel (COMPUTE_COUNT) algorithmic bytes / its device time
 cpu_baseline / --impl reference: the CPU restatement of the reference executor
           (oracle/) on a time-boxed random sample of roots, all host cores (the
@@ -73,13 +74,15 @@ def plan_of(vs, flag):
 
 
 def make_workload(vs, scale=22, edge_factor=16, seed=2, relabel="asc", queries=None):
+    """(relabelled graph, plans, graph in the generator's ids)."""
     t = time.time()
-    g = vs.gen_rmat(scale, edge_factor, 0.57, 0.19, 0.19, seed=seed)
+    raw = vs.gen_rmat(scale, edge_factor, 0.57, 0.19, 0.19, seed=seed)
+    g = raw
     if relabel != "none":
-        g, _ = vs.degree_relabel(g, ascending=(relabel == "asc"))
+        g, _ = vs.degree_relabel(raw, ascending=(relabel == "asc"))
     plans = [plan_of(vs, f) for f in (queries or WORKLOAD["queries"])]
     log(f"graph V={g.V} E={g.E} generated+relabelled in {time.time() - t:.1f}s; plans:", [p.describe() for p in plans])
-    return g, plans
+    return g, plans, raw
 
 
 class Clocks:
@@ -167,6 +170,7 @@ def view_stage_times(vs, eng, g, threads):
         vs.materialize_view(h, src, 2, 0, threads)
         out["materialize_host_ms"] = (time.perf_counter() - t) * 1e3
         import torch
+        eng.set_option("relabel", 0)  # the file's ids, as the reference builds its halos
         eng.upload_graph(h)
         eng.materialize_view(src, 2)  # warm-up
         torch.cuda.synchronize()
@@ -263,7 +267,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    g, plans = make_workload(vs, scale=args.scale, relabel=args.relabel, queries=args.query_flags)
+    g, plans, raw = make_workload(vs, scale=args.scale, relabel=args.relabel, queries=args.query_flags)
     # roots of this rank: a strided share of the vertices (one view per rank)
     from vsgm_b200.shard import allreduce_counts, roots_of_rank
     roots = roots_of_rank(g.V, rank, world)
@@ -332,34 +336,44 @@ def main():
         ms = sum(v for (a, _), v in op_ms.items() if a == pi)
         per_query.append({"query": WORKLOAD["queries"][pi], "count": counts[pi], "device_ms": ms})
 
-    # ---------------- end to end through the C ABI from pinned host buffers
+    # ---------------- end to end through the C ABI from pinned host buffers: the
+    # graph in the generator's ids goes up, is relabelled by degree on the device
+    # (option "relabel", vsgm_upload_graph), every source of this rank (caller ids)
+    # becomes the view's roots (vsgm_graph_view), then match and count read-back
     eng.set_profiling(False)
-    h_rp = torch.from_numpy(g.row_ptrs.view(np.int64)).pin_memory()
-    h_ci = torch.from_numpy(g.cols.view(np.int32)).pin_memory()
+    h_rp = torch.from_numpy(raw.row_ptrs.view(np.int64)).pin_memory()
+    h_ci = torch.from_numpy(raw.cols.view(np.int32)).pin_memory()
     h_src = torch.from_numpy(roots.view(np.int32)).pin_memory()
     L = vs.capi.lib()
     import ctypes as C
-    e2e_ms = []
+    eng.set_option("relabel", 0 if args.relabel == "none" else 1)
+    if args.relabel == "desc":
+        raise SystemExit("the end-to-end pass relabels ascending only")
+    e2e_ms, e2e_counts = [], None
     for s in range(1 + args.e2e_steps):
         eng.reset_counts()
         torch.cuda.synchronize()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        vs.capi.check(L.vsgm_transfer_view(eng.h, C.cast(h_rp.data_ptr(), C.POINTER(C.c_uint64)), C.cast(h_ci.data_ptr(), C.POINTER(C.c_uint32)),
-                                           g.E, C.cast(h_src.data_ptr(), C.POINTER(C.c_uint32)), len(roots)), eng.h)
+        vs.capi.check(L.vsgm_upload_graph(eng.h, C.cast(h_rp.data_ptr(), C.POINTER(C.c_uint64)), C.cast(h_ci.data_ptr(), C.POINTER(C.c_uint32)),
+                                          raw.E), eng.h)
+        vs.capi.check(L.vsgm_graph_view(eng.h, C.cast(h_src.data_ptr(), C.POINTER(C.c_uint32)), len(roots)), eng.h)
         eng.match()
-        got = eng.counts()
+        e2e_counts = eng.counts()
         t1.record(stream)
         torch.cuda.synchronize()
         if s >= 1:  # the first pass is a warm-up
             e2e_ms.append(t0.elapsed_time(t1))
+    if world == 1 and e2e_counts != counts:
+        raise SystemExit(f"end-to-end pass counted {e2e_counts} against {counts}")
     e2e_step = float(np.mean(e2e_ms))
     if world > 1:
         t = torch.tensor([e2e_step], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_step = float(t.item())
     e2e = {"value": matches / (e2e_step / 1e3), "unit": "matches/s", "h2d_bytes_per_step": int(8 * (g.V + 1) + 4 * g.E + 4 * len(roots)),
-           "d2h_bytes_per_step": 8 * len(plans), "ms_per_step": e2e_step, "steps": args.e2e_steps, "warmup": 1}
+           "d2h_bytes_per_step": 8 * len(plans), "ms_per_step": e2e_step, "steps": args.e2e_steps, "warmup": 1,
+           "scope": "generator-id graph from pinned host memory -> device relabel by degree -> all sources -> match -> counts to host"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

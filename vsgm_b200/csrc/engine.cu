@@ -101,7 +101,7 @@ struct vsgm_engine {
   // full graph resident for device-side view materialisation (vsgm_upload_graph)
   uint64_t* g_rp = nullptr;
   uint32_t* g_ci = nullptr;
-  uint64_t g_cols = 0;
+  uint64_t g_cols = 0, g_cap = 0;
   bool relabel = false;         // option "relabel": vsgm_upload_graph orders ids by degree on the device
   uint32_t* g_new = nullptr;    // new id of every caller id of the resident graph (when relabelled)
   // per view: offset of each vertex's first larger neighbour (fused tails with a "> child" condition)
@@ -1449,17 +1449,23 @@ int vsgm_upload_graph(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* 
   return guarded(e, [&] {
     CK(cudaSetDevice(e->device));
     CK(cudaStreamSynchronize(e->stream));
-    if (e->g_rp) CK(cudaFree(e->g_rp));
-    if (e->g_ci) CK(cudaFree(e->g_ci));
-    e->g_rp = nullptr;
-    e->g_ci = nullptr;
-    if (e->g_new) CK(cudaFree(e->g_new));
-    e->g_new = nullptr;
-    CK(cudaMalloc(&e->g_rp, sizeof(uint64_t) * (e->V + 1)));
-    CK(cudaMalloc(&e->g_ci, sizeof(uint32_t) * std::max<uint64_t>(n_cols, 1)));
+    // the buffers of an earlier upload are kept when the new graph fits them
+    if (!e->g_rp) CK(cudaMalloc(&e->g_rp, sizeof(uint64_t) * (e->V + 1)));
+    if (e->g_ci && e->g_cap < n_cols) {
+      CK(cudaFree(e->g_ci));
+      e->g_ci = nullptr;
+    }
+    if (!e->g_ci) {
+      CK(cudaMalloc(&e->g_ci, sizeof(uint32_t) * std::max<uint64_t>(n_cols, 1)));
+      e->g_cap = n_cols;
+    }
+    if (!e->relabel && e->g_new) {
+      CK(cudaFree(e->g_new));
+      e->g_new = nullptr;
+    }
     if (e->relabel) {
       // the caller's graph goes to the arena first, the relabelled one stays resident
-      CK(cudaMalloc(&e->g_new, sizeof(uint32_t) * std::max<uint64_t>(e->V, 1)));
+      if (!e->g_new) CK(cudaMalloc(&e->g_new, sizeof(uint32_t) * std::max<uint64_t>(e->V, 1)));
       Mark m(e->arena);
       e->arena.top = 0;
       uint64_t* t_rp = e->arena.take_n<uint64_t>(e->V + 1, "graph row offsets (caller ids)");
