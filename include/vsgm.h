@@ -262,8 +262,11 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   "tail_merge" (default 0): in the fused tail a heavy child intersects its slice
  *   and its part of N(c) by a merge-path split over the warp's lanes instead of
  *   the walk / gallop;
- *   "c4_heavy" (default 2^16): roots with at least this many wedges are counted by
+ *   "c4_heavy" (default 12289): roots with at least this many wedges are counted by
  *   groups sharing the whole GPU with L2-resident counters (0: every root);
+ *   "c4_hash" (default 1): the other roots keep their counters in a shared-memory
+ *   hash table (a warp per root up to 768 wedges, a block up to 12288; beyond, and
+ *   with 0, one block per root with dense counters in HBM);
  *   "set_reuse" (default 1): a COMPUTE directly followed by the final COMPUTE_COUNT
  *   of a vertex with the same backward lists and conditions (the diamond's tail)
  *   counts the pairs of one intersection instead of intersecting twice;

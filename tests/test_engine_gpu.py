@@ -343,21 +343,25 @@ def test_four_cycle_aggregation_equals_plan(vs, orc, graphs):
     for g in (graphs["rmat7"], graphs["rmat8"], graphs["chunglu"], vs.degree_relabel(graphs["rmat8"])[0],
               vs.degree_relabel(graphs["rmat8"], ascending=False)[0], hub, cycle_graph(vs, 4), complete_graph(vs, 6)):
         want = orc.count(p, g)
-        for agg, heavy in ((1, 1 << 20), (1, 0), (1, 64), (0, 0)):
+        # c4_heavy 0: every root through the group kernels; 2^40: none; c4_hash 0:
+        # light roots through dense counters in HBM instead of shared-memory tables
+        for agg, heavy, hashed in ((1, 1 << 40, 1), (1, 1 << 40, 0), (1, 0, 1), (1, 64, 1), (1, 64, 0), (1, 12289, 1), (0, 0, 1)):
             with vs.Engine(g.V, [p]) as e:
                 e.set_option("c4_aggregate", agg)
-                e.set_option("c4_heavy", heavy)  # 0: every root through the group kernels
+                e.set_option("c4_heavy", heavy)
+                e.set_option("c4_hash", hashed)
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
                 e.match()
-                assert e.counts() == [want], (agg, heavy)
+                assert e.counts() == [want], (agg, heavy, hashed)
     # views: per-view attribution differs, totals do not
     g = graphs["rmat8"]
     bins = (np.arange(g.V) % 3).astype(np.int32)
     assert vs.count_graph(g, [p], views=vs.sources_of_bins(bins, 3)) == [orc.count(p, g)]
     # each view counts the cycles whose largest vertex is one of its sources
-    for heavy in (1 << 18, 0):
+    for heavy, hashed in ((1 << 18, 1), (1 << 18, 0), (0, 1)):
         with vs.Engine(g.V, [p]) as e:
             e.set_option("c4_heavy", heavy)
+            e.set_option("c4_hash", hashed)
             for src in vs.sources_of_bins(bins, 3):
                 e.reset_counts()
                 e.transfer_view(g, src)

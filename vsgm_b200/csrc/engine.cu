@@ -125,7 +125,8 @@ struct vsgm_engine {
     bool lane_merge = false;         // counting kernels: lane-partitioned merge
     bool c4_aggregate = true;        // 4-cycle plans: wedge aggregation instead of the op sequence
     bool set_reuse = true;           // COMPUTE o + COMPUTE_COUNT w over the same set: count pairs of one intersection
-    uint64_t c4_heavy = 1ull << 16;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
+    uint64_t c4_heavy = kC4HashBlockMaxW + 1;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
+    bool c4_hash = true;             // 4-cycle light roots: counters in a shared-memory hash table
     uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
     uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
     bool tail_merge = false;           // fused tail: heavy children by a merge-path split over the lanes
@@ -763,10 +764,11 @@ struct vsgm_engine {
 
   // 4-cycles rooted at the given sources, by wedge aggregation; each cycle is
   // attributed to its largest vertex, the plan attributes it to its smallest:
-  // totals over all sources are the same.  Roots with at least kC4Heavy wedges
-  // (most of the work on skewed graphs) go through the L2-resident group kernels,
-  // the rest through k_c4_aggregate (one root per block).  Threshold: the
-  // per-plan knob c4_heavy (default 2^16 wedges).
+  // totals over all sources are the same.  Roots with at least c4_heavy wedges
+  // (most of the work on skewed graphs; default 12289) go through the L2-resident
+  // group kernels; the others through shared-memory hash tables (knob c4_hash: a
+  // warp per root up to 768 wedges, a block per root up to 12288), and whatever is
+  // left through k_c4_aggregate (one root per block, dense counters in HBM).
   void c4_aggregate(const uint32_t* roots, uint64_t n) {
     const int last = (int)plan->n_ops - 1;
     Mark m(arena);
@@ -784,8 +786,34 @@ struct vsgm_engine {
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_pinned, ctr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    const uint64_t n_heavy = h_pinned[0], n_light = h_pinned[1];
+    const uint64_t n_heavy = h_pinned[0];
+    uint64_t n_light = h_pinned[1];
     uint64_t launches = 2;
+    if (n_light && cur.c4_hash) {
+      // light roots with few wedges: counters in shared-memory hash tables
+      uint32_t* hw = arena.take_n<uint32_t>(n_light, "4-cycle hashed roots");
+      uint32_t* hb = arena.take_n<uint32_t>(n_light, "4-cycle hashed roots");
+      uint32_t* rest = arena.take_n<uint32_t>(n_light, "4-cycle light roots");
+      unsigned long long* hc = arena.take_n<unsigned long long>(4, "4-cycle hash counters");
+      CK(cudaMemsetAsync(hc, 0, 4 * sizeof(unsigned long long), stream));
+      k_c4_split_light<<<grid_threads(n_light), 256, 0, stream>>>(light, n_light, W, kC4HashWarpMaxW, kC4HashBlockMaxW, hw, hb, rest, hc);
+      CK(cudaGetLastError());
+      CK(cudaMemcpyAsync(h_pinned, hc, 3 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+      const uint64_t nw = h_pinned[0], nb = h_pinned[1];
+      const uint32_t* up = upper_offsets();
+      if (nb) {
+        k_c4_hash_block<<<(unsigned)sms, 512, kC4HashBlockSmem, stream>>>(d_rp, d_ci, up, hb, nb, hc + 3, d_total);
+        launches++;
+      }
+      if (nw) {
+        k_c4_hash_warp<<<(unsigned)sms * 2, kC4HashWarps * kWarp, kC4HashWarpSmem, stream>>>(d_rp, d_ci, up, hw, nw, d_total);
+        launches++;
+      }
+      CK(cudaGetLastError());
+      light = rest;
+      n_light = h_pinned[2];
+    }
     if (n_light) {
       launches++;
       const uint64_t per_block = 2ull * V * sizeof(uint32_t);
@@ -1370,6 +1398,8 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     CK(cudaFuncSetAttribute(k_clique_large<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueLargeSmem));
     CK(cudaFuncSetAttribute(k_edge_tri_warp<kTriMid>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTriMidSmem));
     CK(cudaFuncSetAttribute(k_edge_tri_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTriLargeSmem));
+    CK(cudaFuncSetAttribute(k_c4_hash_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kC4HashWarpSmem));
+    CK(cudaFuncSetAttribute(k_c4_hash_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kC4HashBlockSmem));
     CK(cudaEventCreate(&e->ev0));
     CK(cudaEventCreate(&e->ev1));
     CK(cudaEventCreate(&e->ev_h0));
@@ -1669,6 +1699,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   if (n == "walk_ratio") {
     if (value < 0 || value > 65535) return engine_fail(e, VSGM_EINVAL, "walk_ratio must be 0..65535");
     for (int k = lo; k < hi; k++) e->knobs[k].walk_ratio = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "c4_hash") {
+    for (int k = lo; k < hi; k++) e->knobs[k].c4_hash = value != 0;
     return VSGM_OK;
   }
   if (n == "c4_heavy") {

@@ -850,6 +850,9 @@ __global__ void k_expand(Frame in, Expand x, const uint64_t* __restrict__ off, u
 // One block per root; each block owns a dense counter array over the ids and a
 // list of the ids it touched, used to sum and reset.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long pairs_of_u32(uint32_t c) { return (unsigned long long)c * (c ? c - 1u : 0u) / 2; }
+__device__ __forceinline__ unsigned long long pairs_of(uint32_t c) { return pairs_of_u32(c); }
+
 __global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ roots,
                                                       uint64_t n_roots, uint64_t V, uint32_t* __restrict__ L_all, uint32_t* __restrict__ touched_all,
                                                       unsigned long long* __restrict__ head, unsigned long long* __restrict__ total) {
@@ -901,6 +904,142 @@ __global__ void __launch_bounds__(256) k_c4_aggregate(const uint64_t* __restrict
   }
 }
 
+// Light roots of the same count with their counters in a shared-memory hash table
+// instead of a dense array over all ids: distinct opposite vertices w are at most
+// the root's wedge count, so a table of capacity C holds any root with at most
+// 3C/4 wedges (linear probing always ends).  Slots a root used are listed and
+// cleared after its sum, so the table starts empty for the next root.
+constexpr uint32_t kC4HashWarpCap = 1024;    // per warp: roots with <= 768 wedges
+constexpr uint32_t kC4HashBlockCap = 16384;  // per block of 16 warps: roots with <= 12288 wedges
+constexpr uint32_t kC4HashWarpMaxW = kC4HashWarpCap / 4 * 3;
+constexpr uint32_t kC4HashBlockMaxW = kC4HashBlockCap / 4 * 3;
+constexpr int kC4HashWarps = 8;
+constexpr size_t kC4HashWarpSmem = (size_t)kC4HashWarps * kC4HashWarpCap * (4 + 4 + 2);
+constexpr size_t kC4HashBlockSmem = (size_t)kC4HashBlockCap * (4 + 4 + 2);
+
+__device__ __forceinline__ void c4_hash_add(uint32_t* keys, uint32_t* cnt, uint16_t* used, unsigned* n_used, uint32_t mask, int shift, uint32_t w) {
+  uint32_t h = (w * 0x9E3779B1u) >> shift;
+  while (true) {
+    const uint32_t k = ((volatile uint32_t*)keys)[h];
+    if (k == w) break;
+    if (k == 0xffffffffu) {
+      const uint32_t old = atomicCAS(keys + h, 0xffffffffu, w);
+      if (old == 0xffffffffu) {
+        used[atomicAdd(n_used, 1u)] = (uint16_t)h;
+        break;
+      }
+      if (old == w) break;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicAdd(cnt + h, 1u);
+}
+
+// sum C(count, 2) over the listed slots and empty them
+__device__ __forceinline__ unsigned long long c4_hash_drain(uint32_t* keys, uint32_t* cnt, const uint16_t* used, unsigned n, unsigned tid, unsigned nthr) {
+  unsigned long long acc = 0;
+  for (unsigned t = tid; t < n; t += nthr) {
+    const uint32_t h = used[t];
+    acc += pairs_of_u32(cnt[h]);
+    cnt[h] = 0;
+    keys[h] = 0xffffffffu;
+  }
+  return acc;
+}
+
+// a warp per root (<= 768 wedges); each lane walks the lower neighbourhoods of
+// its own wedge centres v < u
+__global__ void __launch_bounds__(kC4HashWarps * 32) k_c4_hash_warp(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                                                    const uint32_t* __restrict__ up, const uint32_t* __restrict__ roots, uint64_t n,
+                                                                    unsigned long long* __restrict__ total) {
+  extern __shared__ uint32_t smem[];
+  __shared__ unsigned s_used[kC4HashWarps];
+  const unsigned lane = lane_id(), wid = threadIdx.x / kWarp;
+  uint32_t* keys = smem + (size_t)wid * kC4HashWarpCap;
+  uint32_t* cnt = smem + (size_t)kC4HashWarps * kC4HashWarpCap + (size_t)wid * kC4HashWarpCap;
+  uint16_t* used = (uint16_t*)(smem + 2 * (size_t)kC4HashWarps * kC4HashWarpCap) + (size_t)wid * kC4HashWarpCap;
+  for (uint32_t t = lane; t < kC4HashWarpCap; t += kWarp) {
+    keys[t] = 0xffffffffu;
+    cnt[t] = 0;
+  }
+  if (lane == 0) s_used[wid] = 0;
+  __syncwarp();
+  const int shift = 32 - 10;  // log2(kC4HashWarpCap)
+  unsigned long long acc = 0;
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  for (uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; r < n; r += warps) {
+    const uint32_t u = __ldg(roots + r);
+    const uint64_t ua = __ldg(rp + u), lower = __ldg(up + u);
+    for (uint64_t k = lane; k < lower; k += kWarp) {
+      const uint32_t v = __ldg(ci + ua + k);
+      const uint64_t vz = __ldg(rp + v + 1);
+      for (uint64_t j = __ldg(rp + v); j < vz; j++) {
+        const uint32_t w = __ldg(ci + j);
+        if (w >= u) break;
+        c4_hash_add(keys, cnt, used, &s_used[wid], kC4HashWarpCap - 1, shift, w);
+      }
+    }
+    __syncwarp();
+    acc += c4_hash_drain(keys, cnt, used, s_used[wid], lane, kWarp);
+    __syncwarp();
+    if (lane == 0) s_used[wid] = 0;
+    __syncwarp();
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if (lane == 0 && acc) atomicAdd(total, acc);
+}
+
+// a block per root (<= 12288 wedges): a warp per wedge centre, lanes over its row
+__global__ void __launch_bounds__(512, 1) k_c4_hash_block(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
+                                                          const uint32_t* __restrict__ roots, uint64_t n, unsigned long long* __restrict__ head,
+                                                          unsigned long long* __restrict__ total) {
+  extern __shared__ uint32_t smem[];
+  __shared__ unsigned s_used;
+  __shared__ unsigned long long s_root;
+  __shared__ unsigned long long s_sum[16];
+  uint32_t* keys = smem;
+  uint32_t* cnt = smem + kC4HashBlockCap;
+  uint16_t* used = (uint16_t*)(smem + 2 * kC4HashBlockCap);
+  const unsigned lane = lane_id(), wid = threadIdx.x / kWarp, nwarps = blockDim.x / kWarp;
+  for (uint32_t t = threadIdx.x; t < kC4HashBlockCap; t += blockDim.x) {
+    keys[t] = 0xffffffffu;
+    cnt[t] = 0;
+  }
+  if (threadIdx.x == 0) s_used = 0;
+  const int shift = 32 - 14;  // log2(kC4HashBlockCap)
+  unsigned long long acc = 0;
+  while (true) {
+    if (threadIdx.x == 0) s_root = atomicAdd(head, 1ull);
+    __syncthreads();
+    const unsigned long long r = s_root;
+    if (r >= n) break;
+    const uint32_t u = __ldg(roots + r);
+    const uint64_t ua = __ldg(rp + u), lower = __ldg(up + u);
+    for (uint64_t k = wid; k < lower; k += nwarps) {
+      const uint32_t v = __ldg(ci + ua + k);
+      const uint64_t vz = __ldg(rp + v + 1);
+      for (uint64_t base = __ldg(rp + v); base < vz; base += kWarp) {
+        const uint64_t j = base + lane;
+        const uint32_t w = j < vz ? __ldg(ci + j) : u;
+        if (w < u) c4_hash_add(keys, cnt, used, &s_used, kC4HashBlockCap - 1, shift, w);
+        if (__any_sync(kFull, w >= u)) break;
+      }
+    }
+    __syncthreads();
+    acc += c4_hash_drain(keys, cnt, used, s_used, threadIdx.x, blockDim.x);
+    __syncthreads();
+    if (threadIdx.x == 0) s_used = 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if (lane == 0) s_sum[wid] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (unsigned w = 0; w < nwarps; w++) t += s_sum[w];
+    if (t) atomicAdd(total, t);
+  }
+}
+
 // Heavy roots of the same count.  A root u with many wedges is shared by the whole
 // GPU: a group of G such roots keeps G dense counter arrays (one per root, over the
 // ids below u) small enough to stay in L2, every warp takes one wedge centre v of
@@ -914,7 +1053,7 @@ struct C4Group {
 };
 constexpr int kC4Group = 8;
 
-__device__ __forceinline__ unsigned long long pairs_of(uint32_t c) { return (unsigned long long)c * (c ? c - 1u : 0u) / 2; }
+
 
 // W[u] += wedges that end at u's lower neighbours: for every edge v-u with v < u,
 // the number of neighbours of v below u (u's position in v's sorted row)
@@ -927,6 +1066,24 @@ __global__ void k_c4_wedge_counts(const uint64_t* __restrict__ rp, const uint32_
       const uint32_t u = __ldg(ci + j);
       if (u > v && j > a) atomicAdd(W + u, (unsigned long long)(j - a));
     }
+  }
+}
+
+// light roots by wedge count for the shared-memory hash kernels: wedge-less roots
+// dropped, <= warp_max to hash_w, <= block_max to hash_b, the rest stay in light
+__global__ void k_c4_split_light(const uint32_t* __restrict__ light, uint64_t n, const unsigned long long* __restrict__ W, unsigned long long warp_max,
+                                 unsigned long long block_max, uint32_t* __restrict__ hash_w, uint32_t* __restrict__ hash_b, uint32_t* __restrict__ rest,
+                                 unsigned long long* __restrict__ counters) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = light[i];
+    const unsigned long long w = W[u];
+    if (w == 0) continue;
+    if (w <= warp_max)
+      hash_w[atomicAdd(counters, 1ull)] = u;
+    else if (w <= block_max)
+      hash_b[atomicAdd(counters + 1, 1ull)] = u;
+    else
+      rest[atomicAdd(counters + 2, 1ull)] = u;
   }
 }
 
