@@ -23,6 +23,8 @@
  *                              ThreadCountWithComputedVertex
  *                              src/gpu/gpu_check_constraints_common.h:120-139
  *      COUNT                   src/executor/ops/count.h:16-167
+ *      COMPUTE_PATH_COUNT      src/executor/ops/compute_path_count.h:7-49 (sizes
+ *                              only; never emitted by the reference planner)
  *      conditions              src/gpu/gpu_utils_filter.h:11-23
  *    OpenMP parallelises over roots.
  * 2. oracle_bruteforce: independent ground truth - injective edge-preserving
@@ -172,6 +174,18 @@ static void run(walk_t* w, int i) {
       run(w, i + 1);
       w->cand[u] = c;
       w->clen[u] = n;
+    } break;
+    case VSGM_COMPUTE_PATH_COUNT: {
+      /* src/executor/ops/compute_path_count.h: the candidate set's size per path;
+       * only a COUNT may read it, which reads the size alone */
+      uint64_t n = intersect(w, u, w->buf[i]);
+      const uint32_t* old = w->cand[u];
+      uint64_t oldn = w->clen[u];
+      w->cand[u] = w->buf[i];
+      w->clen[u] = n;
+      run(w, i + 1);
+      w->cand[u] = old;
+      w->clen[u] = oldn;
     } break;
     case VSGM_COMPUTE_COUNT: {
       uint64_t n = intersect(w, u, w->buf[i]);

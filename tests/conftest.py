@@ -62,3 +62,22 @@ def all_plans(vs):
     for k in (3, 4, 5):
         plans += [(f"km{k}_{i}", p) for i, p in enumerate(vs.plan_graphlets(k))]
     return plans
+
+
+def with_path_count(vs, p):
+    """The same plan with its final COMPUTE_COUNT(u) (no computed vertex counted
+    against) split into COMPUTE_PATH_COUNT(u) and a COUNT of u: the op pair the
+    reference's executor runs for it (src/executor/ops/compute_path_count.h,
+    src/executor/ops/count.h); the reference planner itself never emits it."""
+    q = type(p).from_buffer_copy(bytes(p))
+    i = q.n_ops - 1
+    assert q.op_type[i] == vs.capi.COMPUTE_COUNT and q.computed_unmat[i].count == 0
+    u = q.op_vertex[i]
+    q.op_type[i] = vs.capi.COMPUTE_PATH_COUNT
+    q.op_type[i + 1] = vs.capi.COUNT
+    q.op_vertex[i + 1] = q.n_vertices
+    q.materialized[i + 1] = type(q.materialized[i]).from_buffer_copy(bytes(q.materialized[i]))
+    q.computed_unmat[i + 1].count = 1
+    q.computed_unmat[i + 1].v[0] = u
+    q.n_ops += 1
+    return q

@@ -472,3 +472,29 @@ def test_diamond_from_edge_triangles(vs, orc, graphs):
             e.materialize_view(src, p.hop)
             e.match()
             assert e.counts() == [orc.count(p, g, src)], b
+
+
+def test_compute_path_count_op(vs, orc, graphs):
+    """COMPUTE_PATH_COUNT (sizes only) followed by COUNT, level-wise and in the
+    persistent batched launch, equals the oracle; a plan that would read such a
+    vertex's set later is rejected at vsgm_create."""
+    from conftest import with_path_count
+    g = graphs["chunglu"]
+    base = [vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(1), vs.plan_clique(5)]
+    plans = [with_path_count(vs, p) for p in base]
+    want = [orc.count(p, g) for p in base]
+    assert [orc.count(p, g) for p in plans] == want
+    with vs.Engine(g.V, plans, hbm_budget_bytes=1 << 22) as e:
+        e.set_option("clique_bits", 0)
+        e.set_option("c4_aggregate", 0)
+        e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+        e.match()
+        assert e.counts() == want
+        vid = e.add_view(g)
+        e.set_option("hybrid_steps", 0)
+        assert [row[0] for row in e.run_batched([vid])] == want
+    bad = with_path_count(vs, vs.plan_clique(3))
+    bad.op_type[bad.n_ops - 1] = vs.capi.COMPUTE_COUNT  # would read the sizes-only set as a set
+    bad.computed_unmat[bad.n_ops - 1].count = 1
+    with pytest.raises(vs.VsgmError):
+        vs.Engine(g.V, [bad])

@@ -130,3 +130,11 @@ def test_restated_workload_and_golden_plans(vs, orc):
         q = orc.golden_plan(name)
         assert bytes(q)[:C.sizeof(q)] == bytes(p)[:C.sizeof(p)], name
         assert orc.count(q, hr) == orc.count(p, hr)
+
+
+
+def test_oracle_compute_path_count(vs, orc, g):
+    """COMPUTE_PATH_COUNT + COUNT counts what the fused COMPUTE_COUNT counts."""
+    from conftest import with_path_count
+    for p in (vs.plan_clique(3), vs.plan_clique(4), vs.plan_pattern(1), vs.plan_clique(5)):
+        assert orc.count(with_path_count(vs, p), g) == orc.count(p, g)

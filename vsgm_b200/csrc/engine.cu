@@ -368,6 +368,7 @@ struct vsgm_engine {
       case VSGM_COMPUTE: op_compute(i, f, u); break;
       case VSGM_FILTER_COMPUTE: op_filter(i, f, u); break;
       case VSGM_MATERIALIZE: op_materialize(i, f, u); break;
+      case VSGM_COMPUTE_PATH_COUNT: op_path_count(i, f, u); break;
       default: throw OutOfMemory{"execution sequence holds an op this engine does not run"};
     }
   }
@@ -574,6 +575,43 @@ struct vsgm_engine {
       CK(cudaGetLastError());
       end_op(i, 1);
       st->op_outputs[i] += hi - lo;
+      g.cset[u] = set;
+      g.clen[u] = len;
+      st->batches++;
+      process(i + 1, g);
+      a = b;
+    }
+  }
+
+  // COMPUTE_PATH_COUNT: only the size of every path's candidate set of u; the set
+  // addresses stay zero (plans are checked at vsgm_create: no later op reads them)
+  void op_path_count(int i, const Frame& f, int u) {
+    const vsgm_plan& p = *plan;
+    OpDesc d = make_desc(i, p.compute_cond[u]);
+    uint64_t a = 0;
+    while (a < f.P) {
+      const uint64_t room = std::max<uint64_t>(1, level_budget(i) / 12);
+      const uint64_t b = std::min(f.P, a + room);
+      Mark m(arena);
+      Frame g = slice(f, a, b);
+      uint64_t* set = arena.take_n<uint64_t>(g.P, "candidate sets");
+      uint32_t* len = arena.take_n<uint32_t>(g.P, "candidate sizes");
+      CK(cudaMemsetAsync(set, 0, sizeof(uint64_t) * g.P, stream));
+      begin_op();
+      switch (d.nb) {
+#define VSGM_PATHS(NB) \
+  case NB: k_path_count<NB><<<grid_warps(g.P), 256, 0, stream>>>(g, d, d_rp, d_ci, len); break;
+        VSGM_PATHS(1)
+        VSGM_PATHS(2)
+        VSGM_PATHS(3)
+        VSGM_PATHS(4)
+        VSGM_PATHS(5)
+        VSGM_PATHS(6)
+#undef VSGM_PATHS
+        default: throw OutOfMemory{"pattern vertex with no backward neighbour"};
+      }
+      CK(cudaGetLastError());
+      end_op(i, 1);
       g.cset[u] = set;
       g.clen[u] = len;
       st->batches++;
@@ -1092,6 +1130,7 @@ struct vsgm_engine {
       o.u = p.op_vertex[i];
       o.other = -1;
       const vsgm_conds* c = nullptr;
+      if (o.type == VSGM_COMPUTE_PATH_COUNT) o.type = VSGM_COMPUTE;  // the set's size is all a later COUNT reads
       if (o.type == VSGM_COMPUTE || o.type == VSGM_COMPUTE_COUNT) c = &p.compute_cond[o.u];
       if (o.type == VSGM_MATERIALIZE && i > 0) c = &p.materialize_cond[o.u];
       if (o.type == VSGM_FILTER_COMPUTE) c = &p.filter_cond[o.u];
@@ -1378,6 +1417,20 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     const vsgm_plan& p = plans[k];
     if (p.n_vertices < 2 || p.n_vertices > VSGM_MAX_QV || p.n_ops < 2 || p.n_ops > VSGM_MAX_OPS || p.op_type[0] != VSGM_MATERIALIZE)
       return engine_fail(nullptr, VSGM_EINVAL, "malformed plan");
+    // a COMPUTE_PATH_COUNT vertex has sizes only: a later op may count it, never read it
+    for (uint32_t i = 0; i < p.n_ops; i++) {
+      if (p.op_type[i] != VSGM_COMPUTE_PATH_COUNT) continue;
+      const int u = p.op_vertex[i];
+      for (uint32_t j = i + 1; j < p.n_ops; j++) {
+        const vsgm_vgroup& cu = p.computed_unmat[j];
+        bool in_cu = false;
+        for (int q = 0; q < cu.count; q++) in_cu |= cu.v[q] == u;
+        const int t = p.op_type[j];
+        if (((t == VSGM_MATERIALIZE || t == VSGM_FILTER_COMPUTE) && p.op_vertex[j] == u) || (t == VSGM_COMPUTE_COUNT && in_cu) ||
+            (t == VSGM_COUNT && in_cu && cu.count > 1))
+          return engine_fail(nullptr, VSGM_EINVAL, "a COMPUTE_PATH_COUNT vertex is read by a later op (only a COUNT of it may follow)");
+      }
+    }
   }
   vsgm_engine* e = new vsgm_engine();
   e->device = device;

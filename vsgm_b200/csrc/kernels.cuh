@@ -456,6 +456,27 @@ __global__ void k_compute_write(Frame f, OpDesc d, const uint64_t* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// COMPUTE_PATH_COUNT: the size of every path's candidate set, without the set
+// (src/executor/ops/compute_path_count.h: IntersectCount with a unit functor)
+// ---------------------------------------------------------------------------
+template <int NB>
+__global__ void k_path_count(Frame f, OpDesc d, const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint32_t* __restrict__ len) {
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const unsigned lane = lane_id();
+  for (uint64_t p = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; p < f.P; p += warps) {
+    const uint32_t mine = gather_lane(f, d, p);
+    Window w;
+    make_window(d, mine, &w);
+    Lists L;
+    restrict_lists(d, mine, w, rp, ci, &L);
+    uint32_t n = 0;
+    intersect_warp<NB, true>(w, L, ci, d.merge_ratio, [&](bool ok, uint32_t) { n += ok ? 1u : 0u; }, d.lane_merge);
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_down_sync(kFull, n, o);
+    if (lane == 0) len[p] = n;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // COMPUTE_COUNT: count valid candidates (or, with a computed vertex `other`,
 // the candidates of other standing in relation to each) and add to *total.
 // ---------------------------------------------------------------------------
