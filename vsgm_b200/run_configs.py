@@ -205,26 +205,56 @@ def run_c4(args):
 
 
 def run_c5(args):
+    """C5: generate, relabel on the host and (the engine's resident copy) on the
+    device - the two must agree - count the three queries over every source with
+    their device times, and check that 4 interleaved source bins sum to the totals.
+    (Exact parity on a root sample with the hubs: tests/test_configs_gpu.py.)"""
     k = args.scale_down
     t = time.perf_counter()
-    g = wl.social_chung_lu(V=65_000_000 // k, edges=1_800_000_000 // k)
-    g, _ = degree_relabel(g, ascending=True)
+    raw = wl.social_chung_lu(V=65_000_000 // k, edges=1_800_000_000 // k)
     t_gen = time.perf_counter() - t
+    t = time.perf_counter()
+    g, new_of_old = degree_relabel(raw, ascending=True)
+    t_host_relabel = time.perf_counter() - t
     plans = [plan_clique(3), plan_clique(4), plan_pattern(4)]
-    counts, per, wall = _match_all(g, plans)
-    # the same totals over 4 interleaved source bins
-    bins = [np.arange(b, g.V, 4, dtype=np.uint32) for b in range(4)]
+    out = {"config": "c5", "graph": f"Chung-Lu V={g.V} E={g.E} (exponent 2.2, max degree 5000, seed 5)", "scale_down": k, "gen_s": t_gen,
+           "host_relabel_s": t_host_relabel, "queries": ["-kc 3", "-kc 4", "-p 4"]}
+    print(json.dumps({"progress": out}), flush=True)
     with Engine(g.V, plans) as e:
-        e.upload_graph(g)  # resident once; every bin is matched over it (no halo needed)
+        e.set_option("relabel", 1)
         t = time.perf_counter()
-        for b in bins:
-            e.graph_view(b)
+        e.upload_graph(raw)
+        out["upload_and_device_relabel_s"] = time.perf_counter() - t
+        e.graph_view(np.arange(g.V, dtype=np.uint32))
+        r = e.read_view()
+        out["device_relabel_equals_host"] = bool(np.array_equal(r.row_ptrs, g.row_ptrs) and np.array_equal(r.cols, g.cols))
+        del r
+        e.set_profiling(True)
+        counts, per = [], []
+        for i in range(len(plans)):
+            e.set_option("only_plan", i)
+            e.reset_counts()
+            t = time.perf_counter()
             e.match()
-        bins_wall = time.perf_counter() - t
-        tot = e.counts()
-    return {"config": "c5", "graph": f"Chung-Lu V={g.V} E={g.E} (exponent 2.2, max degree 5000, seed 5)", "scale_down": k, "gen_s": t_gen,
-            "queries": ["-kc 3", "-kc 4", "-p 4"], "counts": counts, "device_ms": per, "wall_ms": wall * 1e3,
-            "bins_total_equal": tot == counts, "bins_wall_ms": bins_wall * 1e3}
+            wall = time.perf_counter() - t
+            counts.append(e.counts()[i])
+            s = e.stats(i)
+            per.append({"query": out["queries"][i], "count": counts[-1], "device_ms": sum(s.op_ms[j] for j in range(plans[i].n_ops)),
+                        "wall_ms": wall * 1e3})
+            print(json.dumps({"progress": per[-1]}), flush=True)
+        e.set_option("only_plan", -1)
+        e.set_profiling(False)
+        out["per_query"] = per
+        out["counts"] = counts
+        # the same totals over 4 interleaved source bins (caller ids)
+        e.reset_counts()
+        t = time.perf_counter()
+        for b in range(4):
+            e.graph_view(np.arange(b, g.V, 4, dtype=np.uint32))
+            e.match()
+        out["bins_wall_ms"] = (time.perf_counter() - t) * 1e3
+        out["bins_total_equal"] = e.counts() == counts
+    return out
 
 
 def main(argv=None):
