@@ -127,6 +127,29 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
  * buffers may be reused as soon as the call returns. */
 int vsgm_transfer_view(vsgm_engine* e, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t n_cols, const uint32_t* sources, uint64_t n_sources);
 
+/* PipelineExecutor::Transfer overlapped with matching (the reference copies
+ * synchronously, src/executor/pipeline_executor.h:64-81).  The view travels in
+ * compact form: the ascending ids of its vertices with a non-empty row
+ * (vertices[n_vertices]) and their offsets into cols (offsets[n_vertices+1],
+ * offsets[0] = 0) - 12 bytes per row of the view instead of 8 per vertex of the
+ * graph; vsgm_view_compact derives it from a full-V view.  The copies go to the
+ * engine's second view buffer on its copy stream and the call returns at once, so
+ * they run while the current view is matched; with host buffers from
+ * vsgm_host_alloc (pinned) they are truly asynchronous.  The host buffers must stay
+ * untouched until vsgm_view_released returns.  vsgm_swap_view makes the prefetched
+ * view the current one (the engine's stream waits for the copies; the host does
+ * not).  One prefetch at a time. */
+int vsgm_prefetch_view(vsgm_engine* e, const uint32_t* vertices, uint64_t n_vertices, const uint64_t* offsets, const uint32_t* cols,
+                       const uint32_t* sources, uint64_t n_sources);
+int vsgm_view_released(vsgm_engine* e);
+int vsgm_swap_view(vsgm_engine* e);
+/* compact form of a full-V view (row_ptrs[V+1], rows contiguous from 0): *n_vertices
+ * rows listed; vertices and offsets need room for V and V+1 entries */
+int vsgm_view_compact(uint64_t V, const uint64_t* row_ptrs, uint32_t* vertices, uint64_t* offsets, uint64_t* n_vertices);
+/* pinned host memory (cudaMallocHost) for view buffers, and its release */
+int vsgm_host_alloc(uint64_t bytes, void** out);
+int vsgm_host_free(void* p);
+
 /* Bind a view already resident in device memory on the engine's device (no
  * copy; the caller keeps it alive until the next transfer or destroy). */
 int vsgm_bind_view_device(vsgm_engine* e, const uint64_t* d_row_ptrs, const uint32_t* d_cols, uint64_t n_cols, const uint32_t* d_sources, uint64_t n_sources);

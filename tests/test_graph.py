@@ -263,3 +263,15 @@ def test_pm_pipeline_fails_cleanly_without_gpu(vs, tmp_path):
     # ... and a halo of the whole graph (-gv 0 / 1) must fit the -m budget
     out = subprocess.run([build.DRIVER, "-f", str(path), "-kc", "3", "-gv", "0", "-m", "1e-9"], capture_output=True, text=True, timeout=120)
     assert out.returncode != 0 and "exceeds -m" in out.stderr
+
+
+def test_view_compact_roundtrip(vs):
+    """The compact view form (vertices with a non-empty row and their offsets)
+    expands back to the full-V row offsets the way the device expands it."""
+    g = vs.gen_rmat(9, 8, seed=4)
+    for src in (np.arange(0, g.V, 5, dtype=np.uint32), np.arange(g.V, dtype=np.uint32), np.zeros(0, np.uint32)):
+        v = vs.materialize_view(g, src, 2)
+        vert, off = vs.view_compact(v)
+        assert off[0] == 0 and off[-1] == v.row_ptrs[-1] and np.all(np.diff(vert.astype(np.int64)) > 0)
+        rp = off[np.searchsorted(vert, np.arange(v.V + 1), side="left")]
+        assert np.array_equal(rp, v.row_ptrs)

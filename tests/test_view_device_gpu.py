@@ -155,3 +155,43 @@ def test_device_relabel_equals_host(vs, orc, graphs):
             e.materialize_view(src, 2)
             e.match()
             assert e.counts() == [orc.count(kc4, h, mapped), orc.c4_by_largest(h, mapped), orc.count(p2, h, mapped)]
+
+
+def test_prefetched_compact_views(vs, orc, graphs):
+    """Views sent in compact form and copied while the previous view is matched
+    (vsgm_prefetch_view / vsgm_swap_view / vsgm_view_released) count what the
+    synchronous full-V transfer counts, bin by bin; pinned host buffers allocate
+    and free."""
+    import ctypes as C
+    g = graphs["rmat8"]
+    plans = [vs.plan_clique(4), vs.plan_pattern(1), vs.plan_pattern(2), vs.plan_pattern(4)]
+    bins = [np.arange(b, g.V, 4, dtype=np.uint32) for b in range(4)]
+    views = [vs.materialize_view(g, src, 2) for src in bins]
+    with vs.Engine(g.V, plans) as e:
+        want = []
+        for v, src in zip(views, bins):
+            e.reset_counts()
+            e.transfer_view(v, src)
+            e.match()
+            want.append(e.counts())
+        got = []
+        e.prefetch_view(views[0], bins[0])
+        e.swap_view()
+        e.view_released()
+        for k in range(4):
+            if k + 1 < 4:
+                e.prefetch_view(views[k + 1], bins[k + 1])  # copies while view k is matched
+            e.reset_counts()
+            e.match()
+            got.append(e.counts())
+            if k + 1 < 4:
+                e.swap_view()
+                e.view_released()
+        assert got == want
+        assert [sum(c[i] for c in got) for i in range(len(plans))] == [orc.count(p, g) for p in plans]
+        with pytest.raises(vs.VsgmError):
+            e.swap_view()  # nothing prefetched
+    p = C.c_void_p()
+    vs.capi.check(vs.capi.lib().vsgm_host_alloc(1 << 20, C.byref(p)))
+    assert p.value
+    vs.capi.check(vs.capi.lib().vsgm_host_free(p))

@@ -193,6 +193,16 @@ def materialize_view(g, sources, hop, root_degree=0, threads=0):
 
 
 # -------------------------------------------------------------------- engine
+def view_compact(g):
+    """Compact form of a full-V view: (ascending vertices with a non-empty row,
+    their offsets into g.cols) - what vsgm_prefetch_view sends."""
+    vert = np.empty(max(g.V, 1), np.uint32)
+    off = np.empty(g.V + 1, np.uint64)
+    n = C.c_uint64()
+    capi.check(_L().vsgm_view_compact(g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(vert, C.c_uint32), capi.ptr(off, C.c_uint64), C.byref(n)))
+    return vert[:n.value].copy(), off[:n.value + 1].copy()
+
+
 class Engine:
     """PipelineExecutor on one GPU: transfer a view, match every plan, read exact counts."""
 
@@ -209,6 +219,24 @@ class Engine:
         self._keep = (view, sources)
         capi.check(_L().vsgm_transfer_view(self.h, capi.ptr(view.row_ptrs, C.c_uint64), capi.ptr(view.cols, C.c_uint32),
                                            view.E, capi.ptr(sources, C.c_uint32), len(sources)), self.h)
+
+    def prefetch_view(self, view, sources):
+        """Start copying a view (in compact form) into the engine's second view
+        buffer; it becomes current at swap_view.  The arrays are kept alive here
+        until view_released."""
+        vert, off = view_compact(view)
+        src = np.ascontiguousarray(sources, dtype=np.uint32)
+        cols = np.ascontiguousarray(view.cols, dtype=np.uint32)
+        self._prefetch_keep = (vert, off, cols, src)
+        capi.check(_L().vsgm_prefetch_view(self.h, capi.ptr(vert, C.c_uint32), len(vert), capi.ptr(off, C.c_uint64), capi.ptr(cols, C.c_uint32),
+                                           capi.ptr(src, C.c_uint32), len(src)), self.h)
+
+    def view_released(self):
+        capi.check(_L().vsgm_view_released(self.h), self.h)
+        self._prefetch_keep = None
+
+    def swap_view(self):
+        capi.check(_L().vsgm_swap_view(self.h), self.h)
 
     def bind_view_device(self, d_row_ptrs, d_cols, n_cols, d_sources, n_sources):
         capi.check(_L().vsgm_bind_view_device(self.h, C.c_void_p(d_row_ptrs), C.c_void_p(d_cols), n_cols,

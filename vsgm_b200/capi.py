@@ -134,6 +134,12 @@ _SIGS = {
     "vsgm_create": (C.c_int, [C.c_int, C.c_uint64, _P(Plan), C.c_int, C.c_uint64, C.c_uint64, _P(C.c_void_p)]),
     "vsgm_transfer_view": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64, _u32p, C.c_uint64]),
     "vsgm_bind_view_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64]),
+    "vsgm_prefetch_view": (C.c_int, [C.c_void_p, _u32p, C.c_uint64, _u64p, _u32p, _u32p, C.c_uint64]),
+    "vsgm_view_released": (C.c_int, [C.c_void_p]),
+    "vsgm_swap_view": (C.c_int, [C.c_void_p]),
+    "vsgm_view_compact": (C.c_int, [C.c_uint64, _u64p, _u32p, _u64p, _u64p]),
+    "vsgm_host_alloc": (C.c_int, [C.c_uint64, _P(C.c_void_p)]),
+    "vsgm_host_free": (C.c_int, [C.c_void_p]),
     "vsgm_upload_graph": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64]),
     "vsgm_materialize_view": (C.c_int, [C.c_void_p, _u32p, C.c_uint64, C.c_int, C.c_uint64]),
     "vsgm_graph_view": (C.c_int, [C.c_void_p, _u32p, C.c_uint64]),

@@ -212,6 +212,22 @@ int vsgm_random_pattern(int n_min, int n_max, double p, uint64_t seed, uint64_t*
   return VSGM_OK;
 }
 
+int vsgm_view_compact(uint64_t V, const uint64_t* row_ptrs, uint32_t* vertices, uint64_t* offsets, uint64_t* n_vertices) {
+  if (!row_ptrs || !vertices || !offsets || !n_vertices) return fail(VSGM_EINVAL, "null argument");
+  uint64_t n = 0;
+  offsets[0] = 0;
+  for (uint64_t v = 0; v < V; v++) {
+    const uint64_t d = row_ptrs[v + 1] - row_ptrs[v];
+    if (!d) continue;
+    if (row_ptrs[v] != offsets[n]) return fail(VSGM_EINVAL, "row_ptrs[0] must be 0 and rows contiguous");
+    vertices[n] = (uint32_t)v;
+    offsets[n + 1] = offsets[n] + d;
+    n++;
+  }
+  *n_vertices = n;
+  return VSGM_OK;
+}
+
 int vsgm_view_materialize(uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, const uint32_t* sources, uint64_t n_sources, int hop,
                           uint64_t root_degree, int threads, uint64_t* view_row_ptrs, uint32_t* view_cols, uint64_t cols_cap, uint64_t* n_cols) {
   if (!row_ptrs || !view_row_ptrs || !n_cols || (n_sources && !sources) || hop < 1) return fail(VSGM_EINVAL, "bad view arguments");

@@ -81,6 +81,16 @@ struct Mark {
 
 }  // namespace
 
+namespace {
+// full-V row offsets of a view sent in compact form: rp[v] = offsets[number of
+// listed vertices below v] (vertices ascending, offsets[0] = 0), rp[V] = the total
+__global__ void k_rows_from_compact(const uint32_t* __restrict__ vert, uint64_t n_vert, const uint64_t* __restrict__ off, uint64_t V,
+                                    uint64_t* __restrict__ rp) {
+  for (uint64_t v = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; v <= V; v += (uint64_t)gridDim.x * blockDim.x)
+    rp[v] = off[lower_bound(vert, 0, n_vert, v)];
+}
+}  // namespace
+
 struct vsgm_engine {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -108,6 +118,18 @@ struct vsgm_engine {
   uint32_t* d_up = nullptr;
   const uint64_t* up_of = nullptr;  // the row_ptrs d_up was computed for
   uint64_t up_cap = 0;
+
+  // second view buffer, filled on the copy stream while the current view is matched
+  // (vsgm_prefetch_view / vsgm_swap_view)
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copy = nullptr;
+  uint64_t* bk_rp = nullptr;
+  uint32_t* bk_ci = nullptr;
+  uint32_t* bk_src = nullptr;
+  uint32_t* bk_vert = nullptr;
+  uint64_t* bk_off = nullptr;
+  uint64_t bk_cols_cap = 0, bk_src_cap = 0, bk_vert_cap = 0, bk_n_cols = 0, bk_n_src = 0;
+  bool bk_pending = false;
 
   Arena arena;
   unsigned long long* d_counts = nullptr;  // [n_plans]
@@ -1444,6 +1466,8 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     CK(cudaSetDevice(device));
     CK(cudaDeviceGetAttribute(&e->sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&e->ev_copy, cudaEventDisableTiming));
     // the clique operator's tiers keep their rows in more than 48 KB of shared memory
     CK(cudaFuncSetAttribute(k_clique_mid<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueMidSmem));
     CK(cudaFuncSetAttribute(k_clique_mid<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueMidSmem));
@@ -1894,6 +1918,91 @@ int vsgm_get_batch_stats(vsgm_engine* e, vsgm_batch_stats* out) {
   return VSGM_OK;
 }
 
+int vsgm_host_alloc(uint64_t bytes, void** out) {
+  if (!out) return engine_fail(nullptr, VSGM_EINVAL, "null argument");
+  *out = nullptr;
+  return guarded(nullptr, [&] { CK(cudaMallocHost(out, std::max<uint64_t>(bytes, 1))); });
+}
+
+int vsgm_host_free(void* p) {
+  return guarded(nullptr, [&] {
+    if (p) CK(cudaFreeHost(p));
+  });
+}
+
+int vsgm_prefetch_view(vsgm_engine* e, const uint32_t* vertices, uint64_t n_vertices, const uint64_t* offsets, const uint32_t* cols,
+                       const uint32_t* sources, uint64_t n_sources) {
+  if (!e || !offsets || (n_vertices && !vertices) || (n_sources && !sources)) return engine_fail(e, VSGM_EINVAL, "null view argument");
+  if (e->bk_pending) return engine_fail(e, VSGM_EINVAL, "a prefetched view is waiting: vsgm_swap_view first");
+  const uint64_t n_cols = offsets[n_vertices];
+  if (n_cols && !cols) return engine_fail(e, VSGM_EINVAL, "null view argument");
+  if (offsets[0] != 0) return engine_fail(e, VSGM_EINVAL, "offsets[0] != 0");
+  for (uint64_t i = 0; i < n_vertices; i++) {
+    if (vertices[i] >= e->V || (i && vertices[i] <= vertices[i - 1])) return engine_fail(e, VSGM_EINVAL, "vertices must ascend and be < V");
+    if (offsets[i + 1] < offsets[i]) return engine_fail(e, VSGM_EINVAL, "offsets must not decrease");
+  }
+  for (uint64_t i = 0; i < n_sources; i++)
+    if (sources[i] >= e->V) return engine_fail(e, VSGM_EINVAL, "source id out of range");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    auto grow = [](auto** p, uint64_t* cap, uint64_t need) {
+      if (*p && *cap >= need) return;
+      if (*p) CK(cudaFree(*p));
+      *p = nullptr;
+      CK(cudaMalloc((void**)p, sizeof(**p) * std::max<uint64_t>(need, 1)));
+      *cap = need;
+    };
+    uint64_t rp_cap = e->bk_rp ? e->V + 1 : 0;
+    grow(&e->bk_rp, &rp_cap, e->V + 1);
+    grow(&e->bk_ci, &e->bk_cols_cap, n_cols);
+    grow(&e->bk_src, &e->bk_src_cap, n_sources);
+    uint64_t off_cap = e->bk_off ? e->bk_vert_cap + 1 : 0;
+    grow(&e->bk_vert, &e->bk_vert_cap, n_vertices);
+    grow(&e->bk_off, &off_cap, n_vertices + 1);
+    cudaStream_t cs = e->copy_stream;
+    if (n_vertices) CK(cudaMemcpyAsync(e->bk_vert, vertices, sizeof(uint32_t) * n_vertices, cudaMemcpyHostToDevice, cs));
+    CK(cudaMemcpyAsync(e->bk_off, offsets, sizeof(uint64_t) * (n_vertices + 1), cudaMemcpyHostToDevice, cs));
+    if (n_cols) CK(cudaMemcpyAsync(e->bk_ci, cols, sizeof(uint32_t) * n_cols, cudaMemcpyHostToDevice, cs));
+    if (n_sources) CK(cudaMemcpyAsync(e->bk_src, sources, sizeof(uint32_t) * n_sources, cudaMemcpyHostToDevice, cs));
+    k_rows_from_compact<<<e->grid_threads(e->V + 1), 256, 0, cs>>>(e->bk_vert, n_vertices, e->bk_off, e->V, e->bk_rp);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(e->ev_copy, cs));
+    e->bk_n_cols = n_cols;
+    e->bk_n_src = n_sources;
+    e->bk_pending = true;
+  });
+}
+
+int vsgm_view_released(vsgm_engine* e) {
+  if (!e) return engine_fail(nullptr, VSGM_EINVAL, "null engine");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    CK(cudaEventSynchronize(e->ev_copy));
+  });
+}
+
+int vsgm_swap_view(vsgm_engine* e) {
+  if (!e) return engine_fail(nullptr, VSGM_EINVAL, "null engine");
+  if (!e->bk_pending) return engine_fail(e, VSGM_EINVAL, "no prefetched view");
+  return guarded(e, [&] {
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamWaitEvent(e->stream, e->ev_copy, 0));  // the engine's stream, not the host, waits for the copies
+    std::swap(e->own_rp, e->bk_rp);
+    std::swap(e->own_ci, e->bk_ci);
+    std::swap(e->cols_cap, e->bk_cols_cap);
+    std::swap(e->own_src, e->bk_src);
+    std::swap(e->src_cap, e->bk_src_cap);
+    e->d_rp = e->own_rp;
+    e->d_ci = e->own_ci;
+    e->d_src = e->own_src;
+    e->n_cols = e->bk_n_cols;
+    e->n_src = e->bk_n_src;
+    e->have_view = true;
+    e->bk_pending = false;
+    e->up_of = nullptr;  // a new view (the same address may come back with other rows)
+  });
+}
+
 int vsgm_destroy(vsgm_engine* e) {
   if (!e) return VSGM_OK;
   cudaSetDevice(e->device);
@@ -1917,6 +2026,14 @@ int vsgm_destroy(vsgm_engine* e) {
   if (e->ev1) cudaEventDestroy(e->ev1);
   if (e->ev_h0) cudaEventDestroy(e->ev_h0);
   if (e->ev_h1) cudaEventDestroy(e->ev_h1);
+  if (e->copy_stream) cudaStreamSynchronize(e->copy_stream);
+  cudaFree(e->bk_rp);
+  cudaFree(e->bk_ci);
+  cudaFree(e->bk_src);
+  cudaFree(e->bk_vert);
+  cudaFree(e->bk_off);
+  if (e->ev_copy) cudaEventDestroy(e->ev_copy);
+  if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return VSGM_OK;
