@@ -11,8 +11,9 @@
 // (vsgm_materialize_view).  In both, producers only hand out bin ids.  With
 // -gv 0 producers materialise the halos on the host into a bounded queue of
 // host buffers, as the reference does, and each consumer uploads them.
-// Either way one consumer per GPU matches every plan and accumulates exact
-// counts.  Without a .vbmap file (the file does not exist) every vertex is a source
+// There the consumers stream the views: a view's copies (in compact form, from a
+// pool of -qs pinned holders) run while the previous view is matched.  Either way
+// one consumer per GPU matches every plan and accumulates exact counts.  Without a .vbmap file (the file does not exist) every vertex is a source
 // of one bin; any other failure to open it is an error.  With -rl 1 (default) the
 // graph is relabelled so that ids ascend with degree before any view is built
 // (inside the timed region; on the device with -gv 1 / 2, on the host with the bins
@@ -61,10 +62,15 @@ double now_us() {
 
 struct View {
   int id = -1;
-  std::vector<uint64_t> row_ptrs;
-  std::vector<uint32_t> cols;
   std::vector<uint32_t> sources;
-  uint64_t n_cols = 0;
+  // -gv 0: a host-built halo in compact form, in pinned buffers of a holder that is
+  // recycled between producers and consumers (the reference's ViewBinBuffer)
+  std::vector<uint64_t> row_ptrs;  // full-V offsets as the materialiser writes them
+  uint32_t* cols = nullptr;        // pinned, cap entries
+  uint32_t* vert = nullptr;        // pinned, V entries
+  uint64_t* off = nullptr;         // pinned, V + 1 entries
+  uint32_t* src = nullptr;         // pinned, V entries
+  uint64_t n_cols = 0, n_vert = 0;
 };
 
 // bounded hand-off between producer and consumer threads
@@ -230,6 +236,21 @@ int main(int argc, char** argv) {
 
   const uint64_t cap = std::min<uint64_t>(E, (uint64_t)(a.mem * 1e9 / sizeof(uint32_t)));
   Queue q(a.qs);
+  // -gv 0: qs pinned holders, handed back through `spare` once their copies are done
+  Queue spare(a.qs);
+  std::vector<View> holders(a.gv == 0 ? a.qs : 0);
+  for (View& h : holders) {
+    h.row_ptrs.resize(V + 1);
+    void *c = nullptr, *vt = nullptr, *o = nullptr, *sr = nullptr;
+    if (vsgm_host_alloc(sizeof(uint32_t) * std::max<uint64_t>(cap, 1), &c) || vsgm_host_alloc(sizeof(uint32_t) * std::max<uint64_t>(V, 1), &vt) ||
+        vsgm_host_alloc(sizeof(uint64_t) * (V + 1), &o) || vsgm_host_alloc(sizeof(uint32_t) * std::max<uint64_t>(V, 1), &sr))
+      return std::fprintf(stderr, "error: pinned view buffers: %s\n", vsgm_last_error()), 1;
+    h.cols = (uint32_t*)c;
+    h.vert = (uint32_t*)vt;
+    h.off = (uint64_t*)o;
+    h.src = (uint32_t*)sr;
+    spare.push(&h);
+  }
   std::atomic<size_t> next{0};
   std::atomic<int> failed{0};
   std::vector<std::vector<uint64_t>> counts(a.cn, std::vector<uint64_t>(plans.size(), 0));
@@ -238,57 +259,104 @@ int main(int argc, char** argv) {
   for (int p = 0; p < a.pn; p++)
     producers.emplace_back([&] {
       for (size_t id; (id = next++) < pool.size();) {
-        View* v = new View();
-        v->id = (int)id;
-        v->sources = pool[id];
         if (a.gv) {  // the consumer builds the halo on its GPU
+          View* v = new View();
+          v->id = (int)id;
+          v->sources = pool[id];
           q.push(v);
           continue;
         }
-        v->row_ptrs.resize(V + 1);
-        v->cols.resize(cap);
-        if (vsgm_view_materialize(V, rp, ci, v->sources.data(), v->sources.size(), hop, root_degree, a.threads, v->row_ptrs.data(), v->cols.data(),
-                                  cap, &v->n_cols)) {
+        View* v = spare.pop();  // a free pinned holder
+        if (!v) break;
+        v->id = (int)id;
+        v->sources = pool[id];
+        std::memcpy(v->src, v->sources.data(), sizeof(uint32_t) * v->sources.size());
+        if (vsgm_view_materialize(V, rp, ci, v->sources.data(), v->sources.size(), hop, root_degree, a.threads, v->row_ptrs.data(), v->cols, cap,
+                                  &v->n_cols) ||
+            vsgm_view_compact(V, v->row_ptrs.data(), v->vert, v->off, &v->n_vert)) {
           std::fprintf(stderr, "error: view %zu: %s\n", id, vsgm_last_error());
           failed = 1;
-          delete v;
+          spare.push(v);
           continue;
         }
         q.push(v);
       }
     });
+  // a view a consumer gives up: pooled holders go back to the producers
+  auto drop = [&](View* v) {
+    if (a.gv == 0)
+      spare.push(v);
+    else
+      delete v;
+  };
   for (int c = 0; c < a.cn; c++)
     consumers.emplace_back([&, c] {
       vsgm_engine* e = nullptr;
       if (vsgm_create(c, V, plans.data(), (int)plans.size(), 0, 0, &e)) {
         std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(nullptr));
         failed = 1;
-        while (View* v = q.pop()) delete v;  // keep producers moving
+        while (View* v = q.pop()) drop(v);  // keep producers moving
         return;
       }
       if (a.gv && a.rl && vsgm_set_option(e, "relabel", 1)) {
         std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(e));
         failed = 1;
-        while (View* v = q.pop()) delete v;
+        while (View* v = q.pop()) drop(v);
         vsgm_destroy(e);
         return;
       }
       if (a.gv && vsgm_upload_graph(e, rp, ci, E)) {
         std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(e));
         failed = 1;
-        while (View* v = q.pop()) delete v;
+        while (View* v = q.pop()) drop(v);
         vsgm_destroy(e);
         return;
       }
-      while (View* v = q.pop()) {
-        int rc = a.gv == 2 ? vsgm_graph_view(e, v->sources.data(), v->sources.size())
-                 : a.gv  ? vsgm_materialize_view(e, v->sources.data(), v->sources.size(), hop, root_degree)
-                         : vsgm_transfer_view(e, v->row_ptrs.data(), v->cols.data(), v->n_cols, v->sources.data(), v->sources.size());
-        delete v;  // the host buffers are free once the transfer returns
-        if (!rc && a.dm) rc = vsgm_match(e);
+      auto fail_here = [&] {
+        std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(e));
+        failed = 1;
+      };
+      if (a.gv) {
+        while (View* v = q.pop()) {
+          int rc = a.gv == 2 ? vsgm_graph_view(e, v->sources.data(), v->sources.size())
+                             : vsgm_materialize_view(e, v->sources.data(), v->sources.size(), hop, root_degree);
+          delete v;
+          if (!rc && a.dm) rc = vsgm_match(e);
+          if (rc) fail_here();
+        }
+      } else {
+        // host-built views: the next view's copies run while the current one is matched
+        auto prefetch = [&](View* v) {
+          return vsgm_prefetch_view(e, v->vert, v->n_vert, v->off, v->cols, v->src, v->sources.size());
+        };
+        auto install = [&](View* v) {  // current := prefetched; the holder goes back to the producers
+          int rc = vsgm_swap_view(e);
+          if (!rc) rc = vsgm_view_released(e);
+          spare.push(v);
+          return rc;
+        };
+        View* v = q.pop();
+        int rc = 0;
+        if (v) {
+          rc = prefetch(v);
+          if (!rc) rc = install(v);
+          else spare.push(v);
+        }
+        while (v) {
+          View* nx = rc ? nullptr : q.pop();
+          if (nx && (rc = prefetch(nx)) != 0) {
+            spare.push(nx);
+            nx = nullptr;
+          }
+          if (!rc && a.dm) rc = vsgm_match(e);
+          if (!nx) break;
+          if (!rc) rc = install(nx);
+          else spare.push(nx);
+          v = nx;
+        }
         if (rc) {
-          std::fprintf(stderr, "error: consumer %d: %s\n", c, vsgm_engine_error(e));
-          failed = 1;
+          fail_here();
+          while (View* w = q.pop()) spare.push(w);  // keep producers moving
         }
       }
       vsgm_get_counts(e, counts[c].data());
@@ -303,6 +371,12 @@ int main(int argc, char** argv) {
     uint64_t s = 0;
     for (int c = 0; c < a.cn; c++) s += counts[c][i];
     std::printf("total count for query %zu: %llu\n", i, (unsigned long long)s);
+  }
+  for (View& h : holders) {
+    vsgm_host_free(h.cols);
+    vsgm_host_free(h.vert);
+    vsgm_host_free(h.off);
+    vsgm_host_free(h.src);
   }
   vsgm_free(rp);
   vsgm_free(ci);
