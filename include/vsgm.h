@@ -299,6 +299,9 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   the persistent launch with this per-task step bound and counts the pairs it
  *   stopped again with the level-wise engine on their resident view (0: the
  *   persistent launch alone, unbounded);
+ *   "streams" (engine-wide, default 4): the pairs a hybrid batched run recounts
+ *   level-wise run this many at a time, each on its own stream and host thread with
+ *   a slice of the engine's working memory (1: one after the other);
  *   "root_stride" (engine-wide, default 1): match only every k-th source of the view
  *   (the autotuner's samples; counts are then those of the sample);
  *   "only_plan" (engine-wide, default -1): vsgm_match runs only this plan.

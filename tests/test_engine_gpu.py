@@ -154,8 +154,11 @@ def test_batched_persistent_run_matches_oracle(vs, orc, graphs):
         assert st.launches == 1 and st.tasks >= len(plans) * len(views) and st.level_pairs == 0
         # hybrid: pairs whose tasks exceed the step bound are counted level-wise
         e.set_option("hybrid_steps", 1)
-        every = e.run_batched(ids)
+        every = e.run_batched(ids)  # every pair recounted level-wise, 4 at a time on their own streams
         assert e.batch_stats().level_pairs == len(plans) * len(views)
+        e.set_option("streams", 1)
+        assert e.run_batched(ids) == every  # one after the other
+        e.set_option("streams", 4)
         e.set_option("hybrid_steps", 1 << 17)
         default = e.run_batched(ids)
         # an explicit pair list gives the same counts as the cross product

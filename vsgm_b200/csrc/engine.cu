@@ -18,12 +18,15 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "clique.cuh"
@@ -159,6 +162,9 @@ struct vsgm_engine {
   Knobs cur;
   uint64_t root_stride = 1;  // >1: match only every root_stride-th source (autotuning samples)
   uint64_t hybrid_steps = 1ull << 14;  // vsgm_run_batched: pairs whose tasks exceed this many steps rerun level-wise (0: never)
+  int streams = 4;                     // those reruns run on this many streams at once (host threads, one helper engine each)
+  std::vector<vsgm_engine*> helpers;   // helper engines: own stream, counters, statistics; the resident views and arena slices are ours
+  bool helper = false;                 // this engine is a helper: its views and arena belong to its parent
   int only_plan = -1;        // >=0: vsgm_match runs this plan only
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEvent_t ev_h0 = nullptr, ev_h1 = nullptr;  // around a hybrid batched run
@@ -1299,15 +1305,71 @@ struct vsgm_engine {
     std::vector<uint32_t> ovf((size_t)n_plans * n_views, 0);
     run_batched(view_ids, n_views, plan_ids, n_plans, counts, nullptr, hybrid_steps, ovf.data(), mask);
     vsgm_batch_stats bs = bstats;
+    std::vector<std::pair<int, int>> rerun;  // (plan index, view index) the persistent launch stopped
     for (int p = 0; p < n_plans; p++)
-      for (int v = 0; v < n_views; v++) {
-        const size_t k = (size_t)p * n_views + v;
-        if (!ovf[k]) continue;
-        counts[k] = run_resident(view_ids[v], plan_ids[p]);
+      for (int v = 0; v < n_views; v++)
+        if (ovf[(size_t)p * n_views + v]) rerun.push_back({p, v});
+    const int K = (int)std::min<size_t>((size_t)std::max(1, streams), rerun.size());
+    if (K <= 1) {
+      for (auto [p, v] : rerun) {
+        counts[(size_t)p * n_views + v] = run_resident(view_ids[v], plan_ids[p]);
         const vsgm_plan_stats& st = stats[plan_ids[p]];
         for (uint32_t i = 0; i < plans[plan_ids[p]].n_ops; i++) bs.launches += st.op_launches[i];
         bs.level_pairs++;
       }
+    } else {
+      // K helper engines on their own streams, each with a slice of our arena, take
+      // the pairs from a shared index (heaviest pairs are not known in advance)
+      CK(cudaStreamSynchronize(stream));
+      const auto t0 = std::chrono::steady_clock::now();
+      const size_t slice = (arena.cap / (size_t)K) & ~(size_t)255;
+      while ((int)helpers.size() < K) helpers.push_back(make_helper());
+      std::atomic<size_t> next{0};
+      std::vector<std::string> errs(K);
+      std::vector<uint64_t> launches(K, 0);
+      std::vector<std::thread> th;
+      for (int k = 0; k < K; k++) {
+        vsgm_engine* h = helpers[k];
+        h->knobs = knobs;
+        h->profiling = profiling;
+        h->rviews = rviews;
+        h->arena.base = arena.base + (size_t)k * slice;
+        h->arena.cap = slice;
+        h->arena.top = h->arena.peak = 0;
+        th.emplace_back([&, h, k] {
+          try {
+            CK(cudaSetDevice(device));
+            for (size_t i; (i = next++) < rerun.size();) {
+              const auto [p, v] = rerun[i];
+              counts[(size_t)p * n_views + v] = h->run_resident(view_ids[v], plan_ids[p]);
+              const vsgm_plan_stats& st = h->stats[plan_ids[p]];
+              for (uint32_t j = 0; j < plans[plan_ids[p]].n_ops; j++) launches[k] += st.op_launches[j];
+            }
+          } catch (const CudaError& c) {
+            errs[k] = std::string("CUDA error ") + cudaGetErrorString(c.code) + " in " + c.what;
+          } catch (const OutOfMemory& o) {
+            errs[k] = o.what;
+          } catch (const std::exception& x) {
+            errs[k] = x.what();
+          }
+        });
+      }
+      for (auto& t : th) t.join();
+      for (const auto& m : errs)
+        if (!m.empty()) throw std::runtime_error("concurrent rerun: " + m);
+      for (uint64_t l : launches) bs.launches += l;
+      bs.level_pairs += rerun.size();
+      if (profiling) {
+        // the helpers' streams are not ours: the persistent launch's events plus host time of the reruns
+        CK(cudaEventRecord(ev_h1, stream));
+        CK(cudaEventSynchronize(ev_h1));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ev_h0, ev_h1));
+        bs.ms = ms + std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        bstats = bs;
+        return;
+      }
+    }
     if (profiling) {
       CK(cudaEventRecord(ev_h1, stream));
       CK(cudaEventSynchronize(ev_h1));
@@ -1316,6 +1378,48 @@ struct vsgm_engine {
       bs.ms = ms;
     }
     bstats = bs;
+  }
+
+  // A helper engine for concurrent reruns: same device, plans and knobs; its own
+  // stream, events, counters and pinned staging; views and arena lent per run.
+  vsgm_engine* make_helper() {
+    vsgm_engine* h = new vsgm_engine();
+    h->helper = true;
+    h->device = device;
+    h->sms = sms;
+    h->V = V;
+    h->plans = plans;
+    h->knobs = knobs;
+    h->totals.assign(plans.size(), 0);
+    h->stats.assign(plans.size(), vsgm_plan_stats{});
+    try {
+      CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+      CK(cudaEventCreate(&h->ev0));
+      CK(cudaEventCreate(&h->ev1));
+      CK(cudaEventCreate(&h->ev_h0));
+      CK(cudaEventCreate(&h->ev_h1));
+      CK(cudaMalloc(&h->d_counts, sizeof(unsigned long long) * (plans.size() + 2)));
+      h->d_bytes = h->d_counts + plans.size();
+      CK(cudaMemset(h->d_counts, 0, sizeof(unsigned long long) * (plans.size() + 2)));
+      CK(cudaMallocHost(&h->h_pinned, 64));
+    } catch (...) {
+      release_helper(h);
+      throw;
+    }
+    return h;
+  }
+
+  static void release_helper(vsgm_engine* h) {
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_counts);
+    cudaFree(h->d_up);
+    if (h->h_pinned) cudaFreeHost(h->h_pinned);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->ev_h0) cudaEventDestroy(h->ev_h0);
+    if (h->ev_h1) cudaEventDestroy(h->ev_h1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
   }
 
   // The level-wise engine on one resident view (the hybrid batched run's heavy
@@ -1801,6 +1905,11 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
     e->only_plan = (int)value;
     return VSGM_OK;
   }
+  if (n == "streams") {
+    if (value < 1 || value > 64) return engine_fail(e, VSGM_EINVAL, "streams must be 1..64");
+    e->streams = (int)value;
+    return VSGM_OK;
+  }
   if (n == "hybrid_steps") {
     if (value < 0) return engine_fail(e, VSGM_EINVAL, "hybrid_steps must be >= 0");
     e->hybrid_steps = (uint64_t)value;
@@ -2006,6 +2115,8 @@ int vsgm_swap_view(vsgm_engine* e) {
 int vsgm_destroy(vsgm_engine* e) {
   if (!e) return VSGM_OK;
   cudaSetDevice(e->device);
+  for (vsgm_engine* h : e->helpers) vsgm_engine::release_helper(h);
+  e->helpers.clear();
   if (e->stream) cudaStreamSynchronize(e->stream);
   cudaFree(e->arena.base);
   cudaFree(e->d_counts);
