@@ -67,3 +67,16 @@ def test_chosen_plans_count_exactly(setup):
         order, _ = model.choose_verified(base, sampler, 0, k=4)
         chosen = vs.plan_reorder(base, order)
         assert vs.count_graph(g, [chosen]) == vs.count_graph(g, [base])
+
+
+def test_plan_error_on_held_out_pairs(setup):
+    """The plain engine judges the network: on held-out pairs its predicted log
+    intermediate sizes are compared with the measured ones of up to 8 orders per
+    pair; the ranking must beat chance and correlate with the measurement."""
+    vs, lp, views, pats, sampler, model, losses, held = setup
+    X, Y, M, _ = lp.make_examples(sampler, pats, held, orders_per_pair=8, seed=2)
+    err = lp.plan_error(model.predict(X), Y, M)
+    print("plan error on held-out pairs:", err)
+    assert err["pairs"] == len(held)
+    assert err["top1"] > err["top1_chance"]
+    assert err["spearman"] is not None and err["spearman"] > 0.3

@@ -154,6 +154,32 @@ def make_examples(sampler, patterns, pairs, orders_per_pair=8, seed=0):
     return np.array(X), np.array(Y), np.array(M), meta
 
 
+def plan_error(pred, Y, M):
+    """The network judged against measured costs on examples it was not trained on:
+    pred / Y / M are predicted log intermediate sizes, measured ones (plan_cost, from
+    the plain engine's per-op partial-match counts) and the mask of measured orders,
+    one row per (pattern, view) pair.  Returns the mean absolute error in log units
+    over every measured (pair, order), the share of pairs whose predicted cheapest
+    measured order is the measured cheapest (and what chance gives), and the mean
+    Spearman rank correlation over pairs with at least 3 measured orders."""
+    errs, top1, chance, rhos = [], 0, 0.0, []
+    for p, y, m in zip(pred, Y, M):
+        idx = np.nonzero(m > 0)[0]
+        if len(idx) == 0:
+            continue
+        errs.extend(np.abs(p[idx] - y[idx]).tolist())
+        top1 += int(idx[np.argmin(p[idx])] == idx[np.argmin(y[idx])])
+        chance += 1.0 / len(idx)
+        if len(idx) >= 3:
+            rp = np.argsort(np.argsort(p[idx])).astype(np.float64)
+            ry = np.argsort(np.argsort(y[idx])).astype(np.float64)
+            if rp.std() > 0 and ry.std() > 0:
+                rhos.append(float(np.corrcoef(rp, ry)[0, 1]))
+    n = sum(1 for m in M if (m > 0).any())
+    return {"pairs": n, "mae_log": float(np.mean(errs)) if errs else None, "top1": top1 / max(n, 1), "top1_chance": chance / max(n, 1),
+            "spearman": float(np.mean(rhos)) if rhos else None}
+
+
 class LearnedPlanner:
     """The MLP, trained and evaluated by the library's own BF16/FP32 kernels."""
 

@@ -196,10 +196,14 @@ def run_c4(args):
         cnt, lvl, ovf = check.evaluate(plans, vi)
         heur += sum(int(x) for x in lvl[0][0][:plans[0].n_ops])
         learned += sum(int(x) for x in lvl[1][0][:plans[1].n_ops])
+    # plan error: predicted against measured log intermediate sizes of several orders
+    # of every held-out pair
+    Xh, Yh, Mh, _ = lp.make_examples(sampler, pats, pairs[cut:], orders_per_pair=8, seed=2)
+    err = lp.plan_error(model.predict(Xh), Yh, Mh)
     if args.save:
         model.save(args.save)
     model.close()
-    return {"config": "c4", "train_pairs": cut, "held_out_pairs": len(pairs) - cut, "examples": int(len(X)), "log_s": t_logs, "train_s": t_train,
+    return {"config": "c4", "plan_error": err, "train_pairs": cut, "held_out_pairs": len(pairs) - cut, "examples": int(len(X)), "log_s": t_logs, "train_s": t_train,
             "loss_first": losses[0], "loss_last": losses[-1], "model_order_used": used,
             "held_out_work": {"heuristic": heur, "learned": learned, "gain": heur / learned if learned else None}}
 
