@@ -848,7 +848,7 @@ struct vsgm_engine {
     CK(cudaMemsetAsync(W, 0, V * sizeof(unsigned long long), stream));
     CK(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), stream));
     k_c4_wedge_counts<<<grid_warps(V), 256, 0, stream>>>(d_rp, d_ci, V, W);
-    k_c4_split<<<grid_threads(n), 256, 0, stream>>>(d_rp, d_ci, roots, n, W, cur.c4_heavy, heavy, centres, light, ctr);
+    k_c4_split<<<grid_threads(n), 256, 0, stream>>>(d_rp, d_ci, roots, n, W, cur.c4_heavy, heavy, centres, light, ctr, profiling ? d_bytes : nullptr);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(h_pinned, ctr, 2 * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));

@@ -1109,11 +1109,16 @@ __global__ void k_c4_split_light(const uint32_t* __restrict__ light, uint64_t n,
 }
 
 // split roots by wedge count; centres[k] = neighbours of heavy root k below it
+// bytes (profiling, may be null): the operator's algorithmic bytes, 8 per wedge (its
+// far end read, its counter updated) and 16 per root (row offsets)
 __global__ void k_c4_split(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ roots, uint64_t n,
                            const unsigned long long* __restrict__ W, unsigned long long threshold, uint32_t* __restrict__ heavy,
-                           uint64_t* __restrict__ centres, uint32_t* __restrict__ light, unsigned long long* __restrict__ counters) {
+                           uint64_t* __restrict__ centres, uint32_t* __restrict__ light, unsigned long long* __restrict__ counters,
+                           unsigned long long* __restrict__ bytes) {
+  unsigned long long b = 0;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t u = roots[i];
+    b += 8ull * W[u] + 16;
     if (W[u] >= threshold) {
       const unsigned long long k = atomicAdd(counters, 1ull);
       heavy[k] = u;
@@ -1121,6 +1126,10 @@ __global__ void k_c4_split(const uint64_t* __restrict__ rp, const uint32_t* __re
     } else {
       light[atomicAdd(counters + 1, 1ull)] = u;
     }
+  }
+  if (bytes) {
+    for (int o = 16; o > 0; o >>= 1) b += __shfl_down_sync(kFull, b, o);
+    if (lane_id() == 0 && b) atomicAdd(bytes, b);
   }
 }
 
