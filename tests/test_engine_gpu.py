@@ -503,3 +503,30 @@ def test_compute_path_count_op(vs, orc, graphs):
     bad.computed_unmat[bad.n_ops - 1].count = 1
     with pytest.raises(vs.VsgmError):
         vs.Engine(g.V, [bad])
+
+
+def test_four_cycle_wide_and_packed_counters(vs, orc):
+    """Heavy 4-cycle roots count with 16-bit counters when they have fewer than 65536
+    neighbours below them and with 32-bit counters otherwise: a wheel whose hub has
+    70000 lower neighbours (each rim vertex closes one cycle through the hub) plus
+    a smaller wheel of 3000, against the oracle, with every root in the groups."""
+    def wheel(n, base):
+        edges = {(base, base + 1 + i) for i in range(n)} | {(base + 1 + i, base + 1 + (i + 1) % n) for i in range(n)}
+        return edges, n + 1
+    e1, n1 = wheel(70000, 0)
+    e2, n2 = wheel(3000, n1)
+    n = n1 + n2
+    rows = [[] for _ in range(n)]
+    for a, b in e1 | e2:
+        rows[a].append(b)
+        rows[b].append(a)
+    rp = np.zeros(n + 1, np.uint64)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    g, _ = vs.degree_relabel(vs.Graph(rp, np.array([x for r in rows for x in sorted(r)], dtype=np.uint32)))
+    want = orc.c4_by_largest_wedges(g)
+    for heavy in (0, 1 << 10, 12289):
+        with vs.Engine(g.V, [vs.plan_pattern(1)]) as e:
+            e.set_option("c4_heavy", heavy)
+            e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+            e.match()
+            assert e.counts() == [want], heavy

@@ -126,6 +126,9 @@ struct vsgm_engine {
   // (vsgm_prefetch_view / vsgm_swap_view)
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_copy = nullptr;
+  // a second compute stream (4-cycle groups alternate between the two), and its fork / join events
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   uint64_t* bk_rp = nullptr;
   uint32_t* bk_ci = nullptr;
   uint32_t* bk_src = nullptr;
@@ -901,30 +904,64 @@ struct vsgm_engine {
       CK(cudaMemcpyAsync(hr.data(), heavy, n_heavy * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
       CK(cudaMemcpyAsync(hc.data(), centres, n_heavy * sizeof(uint64_t), cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
-      // groups of up to kC4Group roots whose counter arrays fit in about 96 MB (L2)
-      const uint64_t stride = (V + 3) & ~3ull;
-      const uint64_t per_root = stride * sizeof(uint32_t);
-      const int G = (int)std::max<uint64_t>(1, std::min<uint64_t>(kC4Group, (96ull << 20) / per_root));
-      std::vector<C4Group> groups;
-      for (uint64_t k = 0; k < n_heavy; k += G) {
-        C4Group g;
-        std::memset(&g, 0, sizeof(g));
-        g.n = (uint32_t)std::min<uint64_t>(G, n_heavy - k);
-        for (uint32_t i = 0; i < g.n; i++) {
-          g.root[i] = hr[k + i];
-          g.vbeg[i + 1] = g.vbeg[i] + hc[k + i];
+      // groups of up to kC4Group roots whose counter arrays fit in about 96 MB (L2):
+      // two buffers of 48 MB on two streams, so that one group's sum pass runs while
+      // the next group adds its wedges; 16-bit counters for roots with fewer than
+      // 65536 neighbours below them (no counter can exceed that), 32-bit for the rest
+      std::vector<uint32_t> pr, wr;
+      std::vector<uint64_t> pc, wc;
+      for (uint64_t k = 0; k < n_heavy; k++) {
+        if (hc[k] < 65536) {
+          pr.push_back(hr[k]);
+          pc.push_back(hc[k]);
+        } else {
+          wr.push_back(hr[k]);
+          wc.push_back(hc[k]);
         }
-        groups.push_back(g);
       }
+      const uint64_t stride_p = (((V + 1) / 2) + 3) & ~3ull, stride_w = (V + 3) & ~3ull;  // words per root
+      const uint64_t buf = 48ull << 20;
+      const int Gp = (int)std::max<uint64_t>(1, std::min<uint64_t>(kC4Group, buf / (stride_p * 4)));
+      const int Gw = (int)std::max<uint64_t>(1, std::min<uint64_t>(kC4Group, buf / (stride_w * 4)));
+      std::vector<C4Group> groups;
+      std::vector<uint8_t> packed;
+      auto make_groups = [&](const std::vector<uint32_t>& r, const std::vector<uint64_t>& c, int G, bool pk) {
+        for (uint64_t k = 0; k < r.size(); k += G) {
+          C4Group g;
+          std::memset(&g, 0, sizeof(g));
+          g.n = (uint32_t)std::min<uint64_t>(G, r.size() - k);
+          for (uint32_t i = 0; i < g.n; i++) {
+            g.root[i] = r[k + i];
+            g.vbeg[i + 1] = g.vbeg[i] + c[k + i];
+          }
+          groups.push_back(g);
+          packed.push_back(pk ? 1 : 0);
+        }
+      };
+      make_groups(pr, pc, Gp, true);
+      make_groups(wr, wc, Gw, false);
+      const uint64_t words = std::max((uint64_t)Gp * stride_p, (uint64_t)Gw * stride_w);
       C4Group* d_groups = arena.take_n<C4Group>(groups.size(), "4-cycle groups");
-      uint32_t* L = arena.take_n<uint32_t>((uint64_t)G * stride, "4-cycle group counters");
+      uint32_t* Lbuf[2] = {arena.take_n<uint32_t>(words, "4-cycle group counters"), arena.take_n<uint32_t>(words, "4-cycle group counters")};
       CK(cudaMemcpyAsync(d_groups, groups.data(), groups.size() * sizeof(C4Group), cudaMemcpyHostToDevice, stream));
-      CK(cudaMemsetAsync(L, 0, (uint64_t)G * per_root, stream));
+      CK(cudaMemsetAsync(Lbuf[0], 0, words * sizeof(uint32_t), stream));
+      CK(cudaMemsetAsync(Lbuf[1], 0, words * sizeof(uint32_t), stream));
+      CK(cudaEventRecord(ev_fork, stream));
+      CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
       const unsigned gw = (unsigned)sms * 8, gs = (unsigned)sms * 4;
       for (size_t i = 0; i < groups.size(); i++) {
-        k_c4_group_wedges<<<gw, 256, 0, stream>>>(d_rp, d_ci, d_groups + i, L, stride);
-        k_c4_group_sum<<<gs, 256, 0, stream>>>(d_groups + i, L, stride, d_total);
+        cudaStream_t st2 = (i & 1) ? aux_stream : stream;  // group i uses buffer i % 2 on stream i % 2
+        uint32_t* L = Lbuf[i & 1];
+        if (packed[i]) {
+          k_c4_group_wedges<true><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_p);
+          k_c4_group_sum<true><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_p, d_total);
+        } else {
+          k_c4_group_wedges<false><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_w);
+          k_c4_group_sum<false><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_w, d_total);
+        }
       }
+      CK(cudaEventRecord(ev_join, aux_stream));
+      CK(cudaStreamWaitEvent(stream, ev_join, 0));
       CK(cudaGetLastError());
       launches += 2 * groups.size();
     }
@@ -1394,6 +1431,9 @@ struct vsgm_engine {
     h->stats.assign(plans.size(), vsgm_plan_stats{});
     try {
       CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+      CK(cudaStreamCreateWithFlags(&h->aux_stream, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
       CK(cudaEventCreate(&h->ev0));
       CK(cudaEventCreate(&h->ev1));
       CK(cudaEventCreate(&h->ev_h0));
@@ -1418,6 +1458,10 @@ struct vsgm_engine {
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->ev_h0) cudaEventDestroy(h->ev_h0);
     if (h->ev_h1) cudaEventDestroy(h->ev_h1);
+    if (h->aux_stream) cudaStreamSynchronize(h->aux_stream);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->aux_stream) cudaStreamDestroy(h->aux_stream);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
   }
@@ -1572,6 +1616,9 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&e->copy_stream, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&e->ev_copy, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&e->aux_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
     // the clique operator's tiers keep their rows in more than 48 KB of shared memory
     CK(cudaFuncSetAttribute(k_clique_mid<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueMidSmem));
     CK(cudaFuncSetAttribute(k_clique_mid<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCliqueMidSmem));
@@ -2145,6 +2192,10 @@ int vsgm_destroy(vsgm_engine* e) {
   cudaFree(e->bk_off);
   if (e->ev_copy) cudaEventDestroy(e->ev_copy);
   if (e->copy_stream) cudaStreamDestroy(e->copy_stream);
+  if (e->aux_stream) cudaStreamSynchronize(e->aux_stream);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_join) cudaEventDestroy(e->ev_join);
+  if (e->aux_stream) cudaStreamDestroy(e->aux_stream);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
   return VSGM_OK;

@@ -1067,12 +1067,12 @@ __global__ void __launch_bounds__(512, 1) k_c4_hash_block(const uint64_t* __rest
 // one root and adds its wedges with fire-and-forget atomics (no return value, so no
 // touched list), and a second pass sums C(L[w], 2) over [0, u) and clears the
 // counters for the next group.
+constexpr int kC4Group = 16;
 struct C4Group {
-  uint32_t n;                  // roots in the group (<= kC4Group)
-  uint32_t root[8];
-  uint64_t vbeg[9];            // prefix of the wedge centres (neighbours below the root) per root
+  uint32_t n;                        // roots in the group (<= kC4Group)
+  uint32_t root[kC4Group];
+  uint64_t vbeg[kC4Group + 1];       // prefix of the wedge centres (neighbours below the root) per root
 };
-constexpr int kC4Group = 8;
 
 
 
@@ -1133,6 +1133,11 @@ __global__ void k_c4_split(const uint64_t* __restrict__ rp, const uint32_t* __re
   }
 }
 
+// kPacked: two 16-bit counters per word (w's counter in the low half of word w/2
+// when w is even, the high half when odd) - used when every root of the group has
+// fewer than 65536 neighbours below it, the bound of any of its counters, so a
+// half never carries into the other; stride is in words either way
+template <bool kPacked>
 __global__ void __launch_bounds__(256) k_c4_group_wedges(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const C4Group* __restrict__ grp,
                                                          uint32_t* __restrict__ L, uint64_t stride) {
   const C4Group& G = *grp;
@@ -1149,23 +1154,35 @@ __global__ void __launch_bounds__(256) k_c4_group_wedges(const uint64_t* __restr
     for (uint64_t base = __ldg(rp + v); base < z; base += kWarp) {
       const uint64_t j = base + lane;
       const uint32_t w = j < z ? __ldg(ci + j) : u;
-      if (w < u) atomicAdd(Lg + w, 1u);
+      if (w < u) {
+        if (kPacked)
+          atomicAdd(Lg + (w >> 1), (w & 1u) ? 0x10000u : 1u);
+        else
+          atomicAdd(Lg + w, 1u);
+      }
       if (__any_sync(kFull, w >= u)) break;
     }
   }
 }
 
+__device__ __forceinline__ unsigned long long pairs_of_halves(uint32_t c) { return pairs_of_u32(c & 0xffffu) + pairs_of_u32(c >> 16); }
+
+template <bool kPacked>
 __global__ void __launch_bounds__(256) k_c4_group_sum(const C4Group* __restrict__ grp, uint32_t* __restrict__ L, uint64_t stride,
                                                       unsigned long long* __restrict__ total) {
   const C4Group& G = *grp;
   unsigned long long acc = 0;
   for (uint32_t g = 0; g < G.n; g++) {
     uint4* Lg = (uint4*)(L + (uint64_t)g * stride);
-    const uint64_t n4 = ((uint64_t)G.root[g] + 3) / 4;  // counters below the root, rounded up (the rest are zero)
+    // counters below the root, rounded up (the rest are zero): 4 per uint4, 8 packed
+    const uint64_t n4 = kPacked ? ((uint64_t)G.root[g] + 7) / 8 : ((uint64_t)G.root[g] + 3) / 4;
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += (uint64_t)gridDim.x * blockDim.x) {
       const uint4 c = Lg[k];
       if (c.x | c.y | c.z | c.w) {
-        acc += pairs_of(c.x) + pairs_of(c.y) + pairs_of(c.z) + pairs_of(c.w);
+        if (kPacked)
+          acc += pairs_of_halves(c.x) + pairs_of_halves(c.y) + pairs_of_halves(c.z) + pairs_of_halves(c.w);
+        else
+          acc += pairs_of(c.x) + pairs_of(c.y) + pairs_of(c.z) + pairs_of(c.w);
         Lg[k] = make_uint4(0u, 0u, 0u, 0u);
       }
     }
