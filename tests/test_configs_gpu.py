@@ -102,6 +102,51 @@ def test_c2_bench_operators_on_hub_roots(vs, orc, rmat22):
             assert e.counts() == want, knobs
 
 
+REF_TOOLS = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_TOOLS, "view_packing")), reason="the reference's view tools are not built")
+def test_c2_on_reference_view_bins(vs, tmp_path):
+    """C2 over the view bins the reference's own offline tools make (compiled from its
+    sources into oracle/_ref): features -h 1, kmeans -k 4 -init 1, view_packing -h 2
+    at a 40 GB budget (one bin) and at 0.45 GB (60 bins; at tighter budgets the
+    reference packer stops on its own vertex-count assertion).  pm_pipeline over those
+    bins gives the whole-graph totals, with the resident graph (-gv 2) and, for the
+    diamond, with host-built halos streamed to the GPU (-gv 0)."""
+    import re
+    import shutil
+    import subprocess
+
+    from vsgm_b200 import build
+    from vsgm_b200 import workloads as wl
+    g, _ = wl.patterns_rmat22()  # the generator's ids, as a user's .bin would have them
+    threads = str(os.cpu_count() or 1)
+    runs = {"40": tmp_path / "m40", "0.45": tmp_path / "m045"}
+    for m, d in runs.items():
+        d.mkdir()
+        vs.write_csr_bin(d / "g.bin", g)
+        if m == "40":
+            subprocess.run([os.path.join(REF_TOOLS, "features"), "-f", "g.bin", "-h", "1"], cwd=d, check=True, capture_output=True, timeout=900)
+            subprocess.run([os.path.join(REF_TOOLS, "kmeans"), "-f", "g.bin.1hop.bin", "-i", "10", "-t", threads, "-k", "4", "-init", "1", "-rc", "1"],
+                           cwd=d, check=True, capture_output=True, timeout=900)
+            shutil.copy(d / "g.bin.1hop.bin.kmeans.4", d / "g.bin.kmeans.1x4")
+        else:
+            shutil.copy(runs["40"] / "g.bin.kmeans.1x4", d / "g.bin.kmeans.1x4")
+        subprocess.run([os.path.join(REF_TOOLS, "view_packing"), "-gf", "g.bin", "-pf", "g.bin.kmeans.1x4", "-h", "2", "-m", m, "-t", "1", "-s", "1",
+                        "-d", "1"], cwd=d, check=True, capture_output=True, timeout=900)
+    assert open(runs["40"] / "g.bin.2.hop.vbmap").readline().strip() == "1"
+    assert int(open(runs["0.45"] / "g.bin.2.hop.vbmap").readline()) > 4
+    for m, d in runs.items():
+        for (flag, val), want in zip((("-kc", "4"), ("-p", "1"), ("-p", "2")), C2_COUNTS):
+            for gv in (("2", "0") if flag == "-p" and val == "2" and m == "0.45" else ("2",)):
+                out = subprocess.run([build.DRIVER, "-f", str(d / "g.bin"), flag, val, "-m", m, "-gv", gv, "-t", threads, "-qs", "2"],
+                                     capture_output=True, text=True, timeout=1200)
+                assert out.returncode == 0, out.stderr
+                assert "loaded view bin partition file" in out.stdout
+                got = int(re.search(r"total count for query 0: (\d+)", out.stdout).group(1))
+                assert got == want, (m, flag, val, gv)
+
+
 @pytest.mark.skipif(os.environ.get("VSGM_LARGE") != "1", reason="65M-vertex graph: set VSGM_LARGE=1")
 def test_c5_large_chung_lu(vs, orc):
     """C5 (65M vertices, ~1.8B edges): the device relabelling equals the host one, a
