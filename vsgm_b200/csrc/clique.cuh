@@ -321,11 +321,16 @@ constexpr size_t kTriLargeSmem = 2ull * kTriLarge * sizeof(uint32_t);
 // the triangles of one root a whose O (d members) and counters cnt[d] (zeroed) are
 // in shared memory; warps take rows wid, wid + nwarps, ...  Counter updates are
 // shared-memory atomics because other warps add column counts concurrently.
+// is_src (byte per vertex): the sources whose out-edges are summed.  A root that is
+// not one of them only feeds the edges (O[i], O[j]) with O[i] a source, so its other
+// rows are skipped (with the sources spread over several GPUs, each does its share).
 __device__ __forceinline__ uint32_t edge_tri_rows(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
-                                                  const uint32_t* O, uint32_t* cnt, uint32_t d, uint32_t wid, uint32_t nwarps, uint32_t* __restrict__ t) {
+                                                  const uint8_t* __restrict__ is_src, bool root_is_src, const uint32_t* O, uint32_t* cnt, uint32_t d,
+                                                  uint32_t wid, uint32_t nwarps, uint32_t* __restrict__ t) {
   const unsigned lane = lane_id();
   uint32_t b = 0;
   for (uint32_t i = wid; i + 1 < d; i += nwarps) {
+    if (!root_is_src && !is_src[O[i]]) continue;
     uint32_t c = 0;
     b += out_row_matches(rp, ci, up, O, d, i, [&](uint32_t j, uint64_t pos) {
       atomicAdd(t + pos, 1u);
@@ -341,8 +346,9 @@ __device__ __forceinline__ uint32_t edge_tri_rows(const uint64_t* __restrict__ r
 // d <= DMAX: a warp per root (roots popped from *head)
 template <uint32_t DMAX>
 __global__ void __launch_bounds__(256) k_edge_tri_warp(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
-                                                       const uint32_t* __restrict__ roots, uint64_t n, unsigned long long* __restrict__ head,
-                                                       uint32_t* __restrict__ t, unsigned long long* __restrict__ bytes) {
+                                                       const uint8_t* __restrict__ is_src, const uint32_t* __restrict__ roots, uint64_t n,
+                                                       unsigned long long* __restrict__ head, uint32_t* __restrict__ t,
+                                                       unsigned long long* __restrict__ bytes) {
   extern __shared__ uint32_t smem[];
   const unsigned lane = lane_id(), wid = threadIdx.x / kWarp;
   uint32_t* O = smem + (size_t)wid * 2 * DMAX;
@@ -361,10 +367,12 @@ __global__ void __launch_bounds__(256) k_edge_tri_warp(const uint64_t* __restric
       cnt[k] = 0;
     }
     __syncwarp();
-    const uint32_t b = edge_tri_rows(rp, ci, up, O, cnt, d, 0, 1, t);
+    const bool a_src = is_src[a] != 0;
+    const uint32_t b = edge_tri_rows(rp, ci, up, is_src, a_src, O, cnt, d, 0, 1, t);
     __syncwarp();
-    for (uint32_t k = lane; k < d; k += kWarp)
-      if (cnt[k]) atomicAdd(t + base + k, cnt[k]);
+    if (a_src)
+      for (uint32_t k = lane; k < d; k += kWarp)
+        if (cnt[k]) atomicAdd(t + base + k, cnt[k]);
     if (bytes && lane == 0) acc_bytes += 16 + 4ull * d + b;
     __syncwarp();
   }
@@ -374,8 +382,9 @@ __global__ void __launch_bounds__(256) k_edge_tri_warp(const uint64_t* __restric
 
 // d <= kTriLarge: a block per root
 __global__ void __launch_bounds__(512, 1) k_edge_tri_block(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
-                                                           const uint32_t* __restrict__ roots, uint64_t n, unsigned long long* __restrict__ head,
-                                                           uint32_t* __restrict__ t, unsigned long long* __restrict__ bytes) {
+                                                           const uint8_t* __restrict__ is_src, const uint32_t* __restrict__ roots, uint64_t n,
+                                                           unsigned long long* __restrict__ head, uint32_t* __restrict__ t,
+                                                           unsigned long long* __restrict__ bytes) {
   extern __shared__ uint32_t smem[];
   __shared__ unsigned long long s_root;
   const unsigned lane = lane_id(), wid = threadIdx.x / kWarp, nwarps = blockDim.x / kWarp;
@@ -395,10 +404,12 @@ __global__ void __launch_bounds__(512, 1) k_edge_tri_block(const uint64_t* __res
       cnt[k] = 0;
     }
     __syncthreads();
-    const uint32_t b = edge_tri_rows(rp, ci, up, O, cnt, d, wid, nwarps, t);
+    const bool a_src = is_src[a] != 0;
+    const uint32_t b = edge_tri_rows(rp, ci, up, is_src, a_src, O, cnt, d, wid, nwarps, t);
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < d; k += blockDim.x)
-      if (cnt[k]) atomicAdd(t + base + k, cnt[k]);
+    if (a_src)
+      for (uint32_t k = threadIdx.x; k < d; k += blockDim.x)
+        if (cnt[k]) atomicAdd(t + base + k, cnt[k]);
     if (bytes && lane == 0) acc_bytes += b + (wid == 0 ? 16 + 4ull * d : 0);
     __syncthreads();  // the next root overwrites O and the counters
   }
@@ -410,12 +421,15 @@ __global__ void __launch_bounds__(512, 1) k_edge_tri_block(const uint64_t* __res
 // neighbours below it (a triangle on (s, v), s < v, has its smallest vertex at s
 // or at a common neighbour below s)
 __global__ void k_tri_mark_roots(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ up,
-                                 const uint32_t* __restrict__ src, uint64_t n, uint8_t* __restrict__ flags) {
+                                 const uint32_t* __restrict__ src, uint64_t n, uint8_t* __restrict__ flags, uint8_t* __restrict__ is_src) {
   const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
   const unsigned lane = lane_id();
   for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < n; i += warps) {
     const uint32_t s = __ldg(src + i);
-    if (lane == 0) set_flag(flags, s);
+    if (lane == 0) {
+      set_flag(flags, s);
+      set_flag(is_src, s);
+    }
     const uint64_t a = __ldg(rp + s), z = a + __ldg(up + s);
     for (uint64_t k = a + lane; k < z; k += kWarp) set_flag(flags, __ldg(ci + k));
   }

@@ -1091,13 +1091,15 @@ struct vsgm_engine {
     Mark m(arena);
     begin_op();
     uint8_t* flags = (uint8_t*)arena.take_n<uint32_t>((V + 3) / 4 + 1, "triangle root flags");
+    uint8_t* is_src = (uint8_t*)arena.take_n<uint32_t>((V + 3) / 4 + 1, "triangle source flags");
     uint32_t* R = arena.take_n<uint32_t>(std::max<uint64_t>(V, 1), "triangle roots");
     CliqueTiers t;
     for (int k = 0; k < 4; k++) t.root[k] = arena.take_n<uint32_t>(std::max<uint64_t>(V, 1), "triangle tier roots");
     t.count = arena.take_n<unsigned long long>(8, "triangle counters");  // 4 tiers, 3 queue heads, the root count
     CK(cudaMemsetAsync(flags, 0, sizeof(uint32_t) * ((V + 3) / 4 + 1), stream));
+    CK(cudaMemsetAsync(is_src, 0, sizeof(uint32_t) * ((V + 3) / 4 + 1), stream));
     CK(cudaMemsetAsync(t.count, 0, 8 * sizeof(unsigned long long), stream));
-    k_tri_mark_roots<<<grid_warps(n), 256, 0, stream>>>(d_rp, d_ci, up, roots, n, flags);
+    k_tri_mark_roots<<<grid_warps(n), 256, 0, stream>>>(d_rp, d_ci, up, roots, n, flags, is_src);
     k_flags_to_list<<<grid_threads(V), 256, 0, stream>>>(flags, V, R, t.count + 7);
     CK(cudaGetLastError());
     const uint64_t nR = read_u64((const uint64_t*)(t.count + 7));
@@ -1120,16 +1122,16 @@ struct vsgm_engine {
     unsigned long long* bytes = profiling ? d_bytes : nullptr;
     uint64_t launches = 5;
     if (nt[2]) {
-      k_edge_tri_block<<<(unsigned)sms, 512, kTriLargeSmem, stream>>>(d_rp, d_ci, up, t.root[2], nt[2], t.count + 4, tri, bytes);
+      k_edge_tri_block<<<(unsigned)sms, 512, kTriLargeSmem, stream>>>(d_rp, d_ci, up, is_src, t.root[2], nt[2], t.count + 4, tri, bytes);
       launches++;
     }
     if (nt[1]) {
-      k_edge_tri_warp<kTriMid><<<(unsigned)sms * 3, 256, kTriMidSmem, stream>>>(d_rp, d_ci, up, t.root[1], nt[1], t.count + 5, tri, bytes);
+      k_edge_tri_warp<kTriMid><<<(unsigned)sms * 3, 256, kTriMidSmem, stream>>>(d_rp, d_ci, up, is_src, t.root[1], nt[1], t.count + 5, tri, bytes);
       launches++;
     }
     if (nt[0]) {
-      k_edge_tri_warp<kTriSmall><<<(unsigned)sms * 8, 256, 8 * 2 * kTriSmall * sizeof(uint32_t), stream>>>(d_rp, d_ci, up, t.root[0], nt[0], t.count + 6,
-                                                                                                       tri, bytes);
+      k_edge_tri_warp<kTriSmall><<<(unsigned)sms * 8, 256, 8 * 2 * kTriSmall * sizeof(uint32_t), stream>>>(d_rp, d_ci, up, is_src, t.root[0], nt[0],
+                                                                                                       t.count + 6, tri, bytes);
       launches++;
     }
     k_diamond_sum<<<grid_warps(n), 256, 0, stream>>>(d_rp, up, roots, n, tri, mode, d_total, bytes);
