@@ -349,14 +349,16 @@ def test_four_cycle_aggregation_equals_plan(vs, orc, graphs):
         want = orc.count(p, g)
         # c4_heavy 0: every root through the group kernels; 2^40: none; c4_hash 0:
         # light roots through dense counters in HBM instead of shared-memory tables
-        for agg, heavy, hashed in ((1, 1 << 40, 1), (1, 1 << 40, 0), (1, 0, 1), (1, 64, 1), (1, 64, 0), (1, 12289, 1), (0, 0, 1)):
+        for agg, heavy, hashed, window in ((1, 1 << 40, 1, 0), (1, 1 << 40, 0, 0), (1, 0, 1, 0), (1, 0, 1, 1), (1, 64, 1, 1), (1, 64, 0, 0),
+                                           (1, 12289, 1, 0), (0, 0, 1, 0)):
             with vs.Engine(g.V, [p]) as e:
                 e.set_option("c4_aggregate", agg)
                 e.set_option("c4_heavy", heavy)
                 e.set_option("c4_hash", hashed)
+                e.set_option("c4_window", window)
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
                 e.match()
-                assert e.counts() == [want], (agg, heavy, hashed)
+                assert e.counts() == [want], (agg, heavy, hashed, window)
     # views: per-view attribution differs, totals do not
     g = graphs["rmat8"]
     bins = (np.arange(g.V) % 3).astype(np.int32)
@@ -525,8 +527,10 @@ def test_four_cycle_wide_and_packed_counters(vs, orc):
     g, _ = vs.degree_relabel(vs.Graph(rp, np.array([x for r in rows for x in sorted(r)], dtype=np.uint32)))
     want = orc.c4_by_largest_wedges(g)
     for heavy in (0, 1 << 10, 12289):
-        with vs.Engine(g.V, [vs.plan_pattern(1)]) as e:
-            e.set_option("c4_heavy", heavy)
-            e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
-            e.match()
-            assert e.counts() == [want], heavy
+        for window in (0, 1):
+            with vs.Engine(g.V, [vs.plan_pattern(1)]) as e:
+                e.set_option("c4_heavy", heavy)
+                e.set_option("c4_window", window)
+                e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+                e.match()
+                assert e.counts() == [want], (heavy, window)

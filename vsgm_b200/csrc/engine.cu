@@ -155,6 +155,7 @@ struct vsgm_engine {
     bool set_reuse = true;           // COMPUTE o + COMPUTE_COUNT w over the same set: count pairs of one intersection
     uint64_t c4_heavy = kC4HashBlockMaxW + 1;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
     bool c4_hash = true;             // 4-cycle light roots: counters in a shared-memory hash table
+    bool c4_window = false;          // 4-cycle heavy roots: the ids just below the root counted in cluster shared memory
     uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
     uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
     bool tail_merge = false;           // fused tail: heavy children by a merge-path split over the lanes
@@ -908,16 +909,34 @@ struct vsgm_engine {
       // two buffers of 48 MB on two streams, so that one group's sum pass runs while
       // the next group adds its wedges; 16-bit counters for roots with fewer than
       // 65536 neighbours below them (no counter can exceed that), 32-bit for the rest
-      std::vector<uint32_t> pr, wr;
+      std::vector<uint32_t> pr, wr, win_roots;
       std::vector<uint64_t> pc, wc;
+      std::vector<uint32_t> plim, wlim;
       for (uint64_t k = 0; k < n_heavy; k++) {
         if (hc[k] < 65536) {
+          // with the window on, the ids [u - kC4Window, u) are counted by the cluster kernel
+          const uint32_t lim = cur.c4_window ? (hr[k] > kC4Window ? hr[k] - kC4Window : 0u) : hr[k];
+          if (cur.c4_window) win_roots.push_back(hr[k]);
+          if (lim == 0) continue;
           pr.push_back(hr[k]);
           pc.push_back(hc[k]);
+          plim.push_back(lim);
         } else {
           wr.push_back(hr[k]);
           wc.push_back(hc[k]);
+          wlim.push_back(hr[k]);
         }
+      }
+      if (!win_roots.empty()) {
+        Mark mw(arena);
+        uint32_t* d_win = arena.take_n<uint32_t>(win_roots.size(), "4-cycle window roots");
+        unsigned long long* whead = arena.take_n<unsigned long long>(1, "4-cycle window queue");
+        CK(cudaMemcpyAsync(d_win, win_roots.data(), win_roots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemsetAsync(whead, 0, sizeof(unsigned long long), stream));
+        const unsigned clusters = std::max(1, sms / kC4WinCtas);
+        k_c4_window<<<clusters * kC4WinCtas, 512, kC4WinSmem, stream>>>(d_rp, d_ci, d_win, win_roots.size(), whead, d_total);
+        CK(cudaGetLastError());
+        launches++;
       }
       const uint64_t stride_p = (((V + 1) / 2) + 3) & ~3ull, stride_w = (V + 3) & ~3ull;  // words per root
       const uint64_t buf = 48ull << 20;
@@ -925,22 +944,25 @@ struct vsgm_engine {
       const int Gw = (int)std::max<uint64_t>(1, std::min<uint64_t>(kC4Group, buf / (stride_w * 4)));
       std::vector<C4Group> groups;
       std::vector<uint8_t> packed;
-      auto make_groups = [&](const std::vector<uint32_t>& r, const std::vector<uint64_t>& c, int G, bool pk) {
+      auto make_groups = [&](const std::vector<uint32_t>& r, const std::vector<uint64_t>& c, const std::vector<uint32_t>& lim, int G, bool pk) {
         for (uint64_t k = 0; k < r.size(); k += G) {
           C4Group g;
           std::memset(&g, 0, sizeof(g));
           g.n = (uint32_t)std::min<uint64_t>(G, r.size() - k);
           for (uint32_t i = 0; i < g.n; i++) {
             g.root[i] = r[k + i];
+            g.lim[i] = lim[k + i];
             g.vbeg[i + 1] = g.vbeg[i] + c[k + i];
           }
           groups.push_back(g);
           packed.push_back(pk ? 1 : 0);
         }
       };
-      make_groups(pr, pc, Gp, true);
-      make_groups(wr, wc, Gw, false);
+      make_groups(pr, pc, plim, Gp, true);
+      make_groups(wr, wc, wlim, Gw, false);
       const uint64_t words = std::max((uint64_t)Gp * stride_p, (uint64_t)Gw * stride_w);
+      if (groups.empty()) goto groups_done;
+      {
       C4Group* d_groups = arena.take_n<C4Group>(groups.size(), "4-cycle groups");
       uint32_t* Lbuf[2] = {arena.take_n<uint32_t>(words, "4-cycle group counters"), arena.take_n<uint32_t>(words, "4-cycle group counters")};
       CK(cudaMemcpyAsync(d_groups, groups.data(), groups.size() * sizeof(C4Group), cudaMemcpyHostToDevice, stream));
@@ -962,8 +984,10 @@ struct vsgm_engine {
       }
       CK(cudaEventRecord(ev_join, aux_stream));
       CK(cudaStreamWaitEvent(stream, ev_join, 0));
-      CK(cudaGetLastError());
       launches += 2 * groups.size();
+      }
+    groups_done:;
+      CK(cudaGetLastError());
     }
     end_op(last, launches);
     st->op_paths[last] += n;
@@ -1630,6 +1654,7 @@ int vsgm_create(int device, uint64_t V, const vsgm_plan* plans, int n_plans, uin
     CK(cudaFuncSetAttribute(k_edge_tri_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTriLargeSmem));
     CK(cudaFuncSetAttribute(k_c4_hash_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kC4HashWarpSmem));
     CK(cudaFuncSetAttribute(k_c4_hash_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kC4HashBlockSmem));
+    CK(cudaFuncSetAttribute(k_c4_window, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kC4WinSmem));
     CK(cudaEventCreate(&e->ev0));
     CK(cudaEventCreate(&e->ev1));
     CK(cudaEventCreate(&e->ev_h0));
@@ -1929,6 +1954,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   if (n == "walk_ratio") {
     if (value < 0 || value > 65535) return engine_fail(e, VSGM_EINVAL, "walk_ratio must be 0..65535");
     for (int k = lo; k < hi; k++) e->knobs[k].walk_ratio = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "c4_window") {
+    for (int k = lo; k < hi; k++) e->knobs[k].c4_window = value != 0;
     return VSGM_OK;
   }
   if (n == "c4_hash") {

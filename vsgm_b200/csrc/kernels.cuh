@@ -20,6 +20,7 @@
 // (src/gpu/gpu_utils_gpsm_bin_search.h:14-130); the set produced is identical.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cstdint>
 
 #include "vsgm_plan.h"
@@ -1071,6 +1072,7 @@ constexpr int kC4Group = 16;
 struct C4Group {
   uint32_t n;                        // roots in the group (<= kC4Group)
   uint32_t root[kC4Group];
+  uint32_t lim[kC4Group];            // wedge ends w < lim are counted here (the root itself, or the start of its window)
   uint64_t vbeg[kC4Group + 1];       // prefix of the wedge centres (neighbours below the root) per root
 };
 
@@ -1147,20 +1149,20 @@ __global__ void __launch_bounds__(256) k_c4_group_wedges(const uint64_t* __restr
   for (uint64_t i = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; i < total; i += warps) {
     uint32_t g = 0;
     while (g + 1 < G.n && i >= G.vbeg[g + 1]) g++;
-    const uint32_t u = G.root[g];
+    const uint32_t u = G.root[g], lim = G.lim[g];
     const uint32_t v = __ldg(ci + __ldg(rp + u) + (i - G.vbeg[g]));  // v < u: the row is sorted
     uint32_t* Lg = L + (uint64_t)g * stride;
     const uint64_t z = __ldg(rp + v + 1);
     for (uint64_t base = __ldg(rp + v); base < z; base += kWarp) {
       const uint64_t j = base + lane;
-      const uint32_t w = j < z ? __ldg(ci + j) : u;
-      if (w < u) {
+      const uint32_t w = j < z ? __ldg(ci + j) : lim;
+      if (w < lim) {
         if (kPacked)
           atomicAdd(Lg + (w >> 1), (w & 1u) ? 0x10000u : 1u);
         else
           atomicAdd(Lg + w, 1u);
       }
-      if (__any_sync(kFull, w >= u)) break;
+      if (__any_sync(kFull, w >= lim)) break;
     }
   }
 }
@@ -1175,7 +1177,7 @@ __global__ void __launch_bounds__(256) k_c4_group_sum(const C4Group* __restrict_
   for (uint32_t g = 0; g < G.n; g++) {
     uint4* Lg = (uint4*)(L + (uint64_t)g * stride);
     // counters below the root, rounded up (the rest are zero): 4 per uint4, 8 packed
-    const uint64_t n4 = kPacked ? ((uint64_t)G.root[g] + 7) / 8 : ((uint64_t)G.root[g] + 3) / 4;
+    const uint64_t n4 = kPacked ? ((uint64_t)G.lim[g] + 7) / 8 : ((uint64_t)G.lim[g] + 3) / 4;
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n4; k += (uint64_t)gridDim.x * blockDim.x) {
       const uint4 c = Lg[k];
       if (c.x | c.y | c.z | c.w) {
@@ -1189,6 +1191,79 @@ __global__ void __launch_bounds__(256) k_c4_group_sum(const C4Group* __restrict_
   }
   for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
   if ((threadIdx.x & (kWarp - 1)) == 0 && acc) atomicAdd(total, acc);
+}
+
+// Heavy roots, the top of their range: a cluster of kC4WinCtas blocks takes one root
+// u at a time and keeps the counters of the ids [u - kC4Window, u) - where most
+// wedges of a heavy root end, the high-degree vertices just below it - as packed
+// 16-bit counters in the distributed shared memory of the cluster (block r holds
+// ids r*kC4WinPerCta ...).  Every warp of the cluster takes wedge centres v, finds
+// the window's start in N(v) and adds its wedges there by shared-memory atomics on
+// the owning block; after a cluster barrier each block sums C(L, 2) over its part
+// and clears it.  The ids below the window stay with the group kernels (lim).  Only
+// roots with fewer than 65536 lower neighbours come here (no counter can overflow).
+constexpr int kC4WinCtas = 4;
+constexpr uint32_t kC4WinWords = 49152;                      // 192 KB of shared memory per block
+constexpr uint32_t kC4WinPerCta = 2 * kC4WinWords;           // ids per block (two per word)
+constexpr uint32_t kC4Window = kC4WinCtas * kC4WinPerCta;    // 393,216 ids below the root
+constexpr size_t kC4WinSmem = (size_t)kC4WinWords * sizeof(uint32_t);
+
+__global__ void __cluster_dims__(kC4WinCtas, 1, 1) __launch_bounds__(512, 1)
+    k_c4_window(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const uint32_t* __restrict__ roots, uint64_t n,
+                unsigned long long* __restrict__ head, unsigned long long* __restrict__ total) {
+  namespace cg = cooperative_groups;
+  extern __shared__ uint32_t win[];
+  __shared__ unsigned long long s_root;
+  __shared__ unsigned long long s_sum[16];
+  cg::cluster_group cluster = cg::this_cluster();
+  const unsigned rank = cluster.block_rank();
+  const unsigned lane = lane_id(), wid = threadIdx.x / kWarp, nwarps = blockDim.x / kWarp;
+  const unsigned gw = rank * nwarps + wid, nw = kC4WinCtas * nwarps;
+  uint32_t* part[kC4WinCtas];
+#pragma unroll
+  for (int r = 0; r < kC4WinCtas; r++) part[r] = cluster.map_shared_rank(win, r);
+  for (uint32_t t = threadIdx.x; t < kC4WinWords; t += blockDim.x) win[t] = 0;
+  unsigned long long acc = 0;
+  while (true) {
+    if (rank == 0 && threadIdx.x == 0) s_root = atomicAdd(head, 1ull);
+    cluster.sync();  // the root is popped and every block's window is clear
+    const unsigned long long r = *cluster.map_shared_rank(&s_root, 0);
+    if (r >= n) break;
+    const uint32_t u = __ldg(roots + r);
+    const uint32_t lo = u > kC4Window ? u - kC4Window : 0u;
+    const uint64_t ua = __ldg(rp + u), uz = __ldg(rp + u + 1);
+    for (uint64_t k = ua + gw; k < uz; k += nw) {
+      const uint32_t v = __ldg(ci + k);
+      if (v >= u) break;  // the row is sorted: the centres below u come first
+      const uint64_t vz = __ldg(rp + v + 1);
+      for (uint64_t base = warp_lower_bound(ci, __ldg(rp + v), vz, lo); base < vz; base += kWarp) {
+        const uint64_t j = base + lane;
+        const uint32_t w = j < vz ? __ldg(ci + j) : u;
+        if (w < u) {
+          const uint32_t x = w - lo;
+          atomicAdd(part[x / kC4WinPerCta] + ((x % kC4WinPerCta) >> 1), (x & 1u) ? 0x10000u : 1u);
+        }
+        if (__any_sync(kFull, w >= u)) break;
+      }
+    }
+    cluster.sync();  // every wedge of u is in the window
+    for (uint32_t t = threadIdx.x; t < kC4WinWords; t += blockDim.x) {
+      const uint32_t c = win[t];
+      if (c) {
+        acc += pairs_of_halves(c);
+        win[t] = 0;
+      }
+    }
+  }
+  cluster.sync();  // no block leaves while another may still read its s_root
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(kFull, acc, o);
+  if (lane == 0) s_sum[wid] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (unsigned w = 0; w < nwarps; w++) t += s_sum[w];
+    if (t) atomicAdd(total, t);
+  }
 }
 
 // ---------------------------------------------------------------------------
