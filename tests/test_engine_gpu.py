@@ -328,8 +328,15 @@ def test_knobs_and_autotuner_keep_counts(vs, orc, graphs):
                 assert e.counts() == want, (walk, ls)
         e.set_option("lane_slice", 16)
         e.set_option("clique_bits", 1)
-        report = autotune(e, len(plans), stride=4)
-        assert [r["plan"] for r in report] == list(range(len(plans)))
+        from vsgm_b200.autotune import TuneCache
+        cache = TuneCache()
+        report = autotune(e, len(plans), stride=4, cache=cache, plans=plans, degrees=g.degrees())
+        assert [r["plan"] for r in report] == list(range(len(plans))) and not any(r["cached"] for r in report)
+        e.match()
+        assert e.counts() == want
+        again = autotune(e, len(plans), stride=4, cache=cache, plans=plans, degrees=g.degrees())  # same view class
+        assert all(r["cached"] for r in again) and [r["best"] for r in again] == [r["best"] for r in report]
+        e.reset_counts()
         e.match()
         assert e.counts() == want
         e.set_option("root_stride", 3)

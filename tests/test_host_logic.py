@@ -105,3 +105,20 @@ def test_strided_shards_partition_the_sources():
         allr = np.sort(np.concatenate(parts))
         assert np.array_equal(allr, src)
         assert max(len(x) for x in parts) - min(len(x) for x in parts) <= 1
+
+
+def test_autotune_view_classes():
+    """The tuner's view signature: degree histograms of the same shape share a class,
+    a heavier tail or a larger hub does not."""
+    import numpy as np
+
+    from vsgm_b200.autotune import TuneCache, view_class
+    rng = np.random.default_rng(1)
+    a = rng.zipf(2.2, size=20000).clip(1, 5000)
+    b = rng.zipf(2.2, size=20000).clip(1, 5000)
+    assert view_class(a) == view_class(b)
+    assert view_class(a) != view_class(np.full(20000, 64))
+    assert view_class(np.full(100, 3)) != view_class(np.concatenate([np.full(99, 3), [100000]]))
+    c = TuneCache()
+    c.put(b"plan", view_class(a), {"fuse_tail": 0})
+    assert c.get(b"plan", view_class(b)) == {"fuse_tail": 0} and c.get(b"other", view_class(b)) is None
