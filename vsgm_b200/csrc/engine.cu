@@ -961,32 +961,30 @@ struct vsgm_engine {
       make_groups(pr, pc, plim, Gp, true);
       make_groups(wr, wc, wlim, Gw, false);
       const uint64_t words = std::max((uint64_t)Gp * stride_p, (uint64_t)Gw * stride_w);
-      if (groups.empty()) goto groups_done;
-      {
-      C4Group* d_groups = arena.take_n<C4Group>(groups.size(), "4-cycle groups");
-      uint32_t* Lbuf[2] = {arena.take_n<uint32_t>(words, "4-cycle group counters"), arena.take_n<uint32_t>(words, "4-cycle group counters")};
-      CK(cudaMemcpyAsync(d_groups, groups.data(), groups.size() * sizeof(C4Group), cudaMemcpyHostToDevice, stream));
-      CK(cudaMemsetAsync(Lbuf[0], 0, words * sizeof(uint32_t), stream));
-      CK(cudaMemsetAsync(Lbuf[1], 0, words * sizeof(uint32_t), stream));
-      CK(cudaEventRecord(ev_fork, stream));
-      CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
-      const unsigned gw = (unsigned)sms * 8, gs = (unsigned)sms * 4;
-      for (size_t i = 0; i < groups.size(); i++) {
-        cudaStream_t st2 = (i & 1) ? aux_stream : stream;  // group i uses buffer i % 2 on stream i % 2
-        uint32_t* L = Lbuf[i & 1];
-        if (packed[i]) {
-          k_c4_group_wedges<true><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_p);
-          k_c4_group_sum<true><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_p, d_total);
-        } else {
-          k_c4_group_wedges<false><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_w);
-          k_c4_group_sum<false><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_w, d_total);
+      if (!groups.empty()) {
+        C4Group* d_groups = arena.take_n<C4Group>(groups.size(), "4-cycle groups");
+        uint32_t* Lbuf[2] = {arena.take_n<uint32_t>(words, "4-cycle group counters"), arena.take_n<uint32_t>(words, "4-cycle group counters")};
+        CK(cudaMemcpyAsync(d_groups, groups.data(), groups.size() * sizeof(C4Group), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemsetAsync(Lbuf[0], 0, words * sizeof(uint32_t), stream));
+        CK(cudaMemsetAsync(Lbuf[1], 0, words * sizeof(uint32_t), stream));
+        CK(cudaEventRecord(ev_fork, stream));
+        CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
+        const unsigned gw = (unsigned)sms * 8, gs = (unsigned)sms * 4;
+        for (size_t i = 0; i < groups.size(); i++) {
+          cudaStream_t st2 = (i & 1) ? aux_stream : stream;  // group i uses buffer i % 2 on stream i % 2
+          uint32_t* L = Lbuf[i & 1];
+          if (packed[i]) {
+            k_c4_group_wedges<true><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_p);
+            k_c4_group_sum<true><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_p, d_total);
+          } else {
+            k_c4_group_wedges<false><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_w);
+            k_c4_group_sum<false><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_w, d_total);
+          }
         }
+        CK(cudaEventRecord(ev_join, aux_stream));
+        CK(cudaStreamWaitEvent(stream, ev_join, 0));
+        launches += 2 * groups.size();
       }
-      CK(cudaEventRecord(ev_join, aux_stream));
-      CK(cudaStreamWaitEvent(stream, ev_join, 0));
-      launches += 2 * groups.size();
-      }
-    groups_done:;
       CK(cudaGetLastError());
     }
     end_op(last, launches);
