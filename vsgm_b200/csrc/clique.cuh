@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(kCliqueLargeWarps * kWarp, 1)
 // count of b plus column count of c) and are added once per root.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kTriSmall = 32;    // warp per root, O and counts in static shared memory
-constexpr uint32_t kTriMid = 256;     // warp per root, 2 KB of shared memory per warp (wider roots: a block, rows over 16 warps)
+constexpr uint32_t kTriMid = 1024;    // warp per root, 8 KB of shared memory per warp (measured: a 256 cut with the block tier above it took -p 2 from 134 to 152 ms)
 constexpr uint32_t kTriLarge = 16384; // block per root, 128 KB of shared memory
 constexpr size_t kTriMidSmem = 8ull * 2 * kTriMid * sizeof(uint32_t);
 constexpr size_t kTriLargeSmem = 2ull * kTriLarge * sizeof(uint32_t);
