@@ -112,6 +112,42 @@ int vsgm_degree_relabel(uint64_t V, const uint64_t* row_ptrs, const uint32_t* co
 int vsgm_view_materialize(uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, const uint32_t* sources, uint64_t n_sources, int hop,
                           uint64_t root_degree, int threads, uint64_t* view_row_ptrs, uint32_t* view_cols, uint64_t cols_cap, uint64_t* n_cols);
 
+/* ------------------------------------------- view-bin tools on the device
+ * The offline chain that produces the .vbmap (features -h 1 -> kmeans ->
+ * view_packing), run on GPU `device` from host buffers, each with exactly the
+ * reference tool's output.  The graph must be undirected with sorted rows. */
+
+/* features -h 1 (src/tools/features.cc:177-201): every row gains its own vertex
+ * in sorted position.  out_row_ptrs has V+1 entries, out_cols E+V. */
+int vsgm_features_1hop(int device, uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, uint64_t* out_row_ptrs, uint32_t* out_cols);
+
+/* kmeans -k K -i max_iter -init 1 [-rc 1] (src/tools/kmeans.cc:54-247, 386-510,
+ * 636-694; cosine similarity, src/tools/kmeans_utils.h:40-160), single level.
+ * The random initialisation is given explicitly: starts[p] (n_starts = the
+ * reference's thread count -t) is the cluster its thread p draws with
+ * std::rand() % K (kmeans.cc:125-141); thread p's vertices p, p+T, ... take
+ * consecutive clusters from there.  With -rc 1 the clusters are renumbered by
+ * the non-zero entries of their centroids, counted for the first
+ * min(K, n_starts) only, as the reference counts them.  Writes the
+ * assignment (V entries, empty clusters removed), the sizes of the n_clusters
+ * non-empty clusters (K entries of space) and *n_clusters.  K <= 128. */
+int vsgm_kmeans(int device, uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, int K, int max_iter, const int32_t* starts, int n_starts,
+                int reorder_centroids, int32_t* assignment, int64_t* cluster_sizes, int32_t* n_clusters);
+
+/* view_packing -s 1 (src/tools/view_packing.cc:141-324, ViewBinPool with one
+ * open bin, src/tools/view_bin.h:22-138): each of the n_seqs sequences
+ * order[seq_offsets[q] .. seq_offsets[q+1]) (one per packing thread -t; their
+ * order built from the partition file as the reference builds it) is packed
+ * next-fit into bins of at most max_bin_size row entries, a source adding the
+ * rows of its (hop-1)-ball not yet in the bin (hop 1..3); then the bins are
+ * merged next-fit by size.  Writes the .vbmap content (bin_of_vertex[V],
+ * *n_bins) and, when bin_sizes is given, the row entries of the first
+ * sizes_cap merged bins (the .vbstat sizes).  A source whose ball alone
+ * exceeds max_bin_size is an error (the reference drops it and fails its own
+ * vertex-count assertion). */
+int vsgm_view_packing(int device, uint64_t V, const uint64_t* row_ptrs, const uint32_t* cols, const uint32_t* order, const uint64_t* seq_offsets,
+                      int n_seqs, int hop, uint64_t max_bin_size, int32_t* bin_of_vertex, int32_t* n_bins, uint64_t* bin_sizes, uint64_t sizes_cap);
+
 /* ------------------------------------------------------------------- engine */
 
 typedef struct vsgm_engine vsgm_engine; /* one per host thread per GPU */

@@ -1,0 +1,92 @@
+"""Host-side pieces of the device view-bin chain and its golden fixture (no GPU).
+
+The fixture (tests/golden/ref_view_tools.npz) is the reference tools' own output;
+here it is checked for internal consistency against definitions that need no GPU:
+the self-loop graph by numpy, every vertex in exactly one packed bin, each bin's
+size within the budget and equal to the row entries of its sources' balls.  The
+helpers that rebuild the reference's inputs are checked too: the random start
+against glibc's rand() in a fresh process, and the packing order from a
+partition file's suffix.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden", "ref_view_tools.npz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+@pytest.mark.parametrize("name", ["rmat", "chunglu"])
+def test_fixture_self_loop_graph(gold, name):
+    rp, ci = gold[f"{name}_rp"], gold[f"{name}_ci"]
+    V = len(rp) - 1
+    rows = [np.sort(np.append(ci[rp[v]:rp[v + 1]], v)) for v in range(V)]
+    np.testing.assert_array_equal(gold[f"{name}_1hop_rp"], np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint64))
+    np.testing.assert_array_equal(gold[f"{name}_1hop_ci"], np.concatenate(rows).astype(np.uint32))
+
+
+def _ball(rp, ci, s, radius):
+    ball, frontier = {s}, [s]
+    for _ in range(radius):
+        nxt = []
+        for x in frontier:
+            for y in ci[rp[x]:rp[x + 1]]:
+                if int(y) not in ball:
+                    ball.add(int(y))
+                    nxt.append(int(y))
+        frontier = nxt
+    return ball
+
+
+@pytest.mark.parametrize("name", ["rmat", "chunglu"])
+def test_fixture_bins_cover_the_vertices_within_budget(gold, name):
+    rp, ci = gold[f"{name}_rp"], gold[f"{name}_ci"]
+    V = len(rp) - 1
+    deg = np.diff(rp).astype(np.int64)
+    cases = gold["pack_cases"]
+    for c in gold[f"{name}_pack_cases"][:3]:
+        hop = int(cases[c][0])
+        bins = gold[f"{name}_pack_{c}_vbmap"]
+        nb = int(gold[f"{name}_pack_{c}_nbins"][0])
+        cap = int(float(gold[f"{name}_pack_{c}_mem"][0]) * 1000 * 1000 * 1000 / 4)
+        assert len(bins) == V and bins.min() == 0 and bins.max() == nb - 1
+        sizes = gold[f"{name}_pack_{c}_sizes"]
+        assert len(sizes) == nb
+        # a merged bin's size is the sum over its packed bins: at least its own
+        # sources' union of balls, and each packed bin is within the budget
+        for b in range(nb):
+            members = np.nonzero(bins == b)[0]
+            union = set()
+            for s in members:
+                union |= _ball(rp, ci, int(s), hop - 1)
+            assert deg[list(union)].sum() <= int(sizes[b])
+        assert all(int(s) <= cap for s in sizes)
+
+
+def test_reference_rand_starts_are_glibc_draws(vs):
+    code = "import ctypes, ctypes.util; c = ctypes.CDLL(ctypes.util.find_library('c')); print([c.rand() for _ in range(5)])"
+    draws = eval(subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, check=True).stdout)
+    for k in (2, 3, 4, 7, 64):
+        np.testing.assert_array_equal(vs.reference_rand_starts(k, 5), np.array(draws) % k)
+
+
+def test_packing_order_follows_the_partition_suffix(vs):
+    part = np.array([1, 0, 3, 2, 1, 0, 2, 3])
+    order, offs = vs.packing_order(part, "1x4", 1)
+    np.testing.assert_array_equal(order, [1, 5, 0, 4, 3, 6, 2, 7])
+    np.testing.assert_array_equal(offs, [0, 8])
+    order, offs = vs.packing_order(part, "4", 4)
+    np.testing.assert_array_equal(order, [1, 5, 0, 4, 3, 6, 2, 7])
+    np.testing.assert_array_equal(offs, [0, 2, 4, 6, 8])
+    order, offs = vs.packing_order(part, "2x2", 2)
+    np.testing.assert_array_equal(offs, [0, 4, 8])
+    with pytest.raises(ValueError):
+        vs.packing_order(part, "4", 1)

@@ -192,6 +192,85 @@ def materialize_view(g, sources, hop, root_degree=0, threads=0):
     return Graph(vrp, vci[:n.value])
 
 
+# ------------------------------------------------- view-bin tools (device)
+def features_1hop(g, device=0):
+    """features -h 1 on the GPU: every row gains its own vertex (src/tools/features.cc:177-201)."""
+    rp = np.empty(g.V + 1, np.uint64)
+    ci = np.empty(g.E + g.V, np.uint32)
+    capi.check(_L().vsgm_features_1hop(device, g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32), capi.ptr(rp, C.c_uint64),
+                                       capi.ptr(ci, C.c_uint32)))
+    return Graph(rp, ci)
+
+
+def reference_rand_starts(k, threads=1):
+    """The clusters the reference's random initialisation draws in a fresh process:
+    std::rand() % k once per thread (kmeans.cc:125-141) from glibc's generator at
+    its default seed 1 (the published additive-feedback recurrence
+    r[i] = r[i-31] + r[i-3], output r >> 1).  With threads > 1 the reference's
+    threads draw in whatever order they start; this gives thread p the p-th draw."""
+    r = [1]
+    for i in range(1, 31):
+        r.append((16807 * r[i - 1]) % 2147483647)
+    r += r[0:3]
+    draws = []
+    for i in range(34, 344 + threads):
+        r.append((r[i - 31] + r[i - 3]) & 0xFFFFFFFF)
+        if i >= 344:
+            draws.append(r[i] >> 1)
+    return np.array([d % k for d in draws], np.int32)
+
+
+def kmeans(g, k, iters=20, starts=None, reorder=False, device=0):
+    """kmeans -k K -i iters -init 1 [-rc 1] on the GPU over the rows of g (use the
+    features_1hop graph, as the reference pipeline does).  starts: the cluster each
+    reference thread draws (default: reference_rand_starts(k, 1), i.e. -t 1).
+    Returns (assignment int32[V], sizes of the non-empty clusters)."""
+    starts = np.ascontiguousarray(reference_rand_starts(k, 1) if starts is None else starts, dtype=np.int32)
+    assign = np.empty(g.V, np.int32)
+    sizes = np.zeros(k, np.int64)
+    n = C.c_int32()
+    capi.check(_L().vsgm_kmeans(device, g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32), k, iters, capi.ptr(starts, C.c_int32),
+                                len(starts), 1 if reorder else 0, capi.ptr(assign, C.c_int32), sizes.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(n)))
+    return assign, sizes[:n.value].copy()
+
+
+def packing_order(partition, suffix, threads):
+    """The source order and per-thread sequences view_packing -o 0 builds from a
+    partition file (src/tools/view_packing.cc:150-190): suffix "K" (K == threads)
+    gives thread t the vertices of cluster t in id order; "AxB" (A == threads)
+    gives thread t clusters t*B .. t*B+B-1 one after the other."""
+    partition = np.asarray(partition)
+    if "x" in suffix:
+        first, second = (int(x) for x in suffix.split("x"))
+    else:
+        first, second = int(suffix), 1
+    if first != threads:
+        raise ValueError(f"partition suffix {suffix!r} needs {first} packing threads, not {threads}")
+    key = partition.astype(np.int64)
+    seqs = [np.nonzero(key // second == t)[0] for t in range(first)]
+    seqs = [s_[np.argsort(key[s_] % second, kind="stable")].astype(np.uint32) for s_ in seqs]
+    order = np.concatenate(seqs).astype(np.uint32) if seqs else np.zeros(0, np.uint32)
+    offsets = np.zeros(len(seqs) + 1, np.uint64)
+    offsets[1:] = np.cumsum([len(x) for x in seqs])
+    return order, offsets
+
+
+def view_packing(g, order, seq_offsets, hop, mem_gb, device=0):
+    """view_packing -h hop -m mem_gb -s 1 on the GPU: returns (bin of every vertex,
+    number of bins, row entries per bin).  The bin size is mem_gb * 1e9 / 4 row
+    entries, computed as the reference computes it."""
+    order = np.ascontiguousarray(order, dtype=np.uint32)
+    seq_offsets = np.ascontiguousarray(seq_offsets, dtype=np.uint64)
+    cap = int(float(mem_gb) * 1000 * 1000 * 1000 / 4)
+    bins = np.empty(g.V, np.int32)
+    nb = C.c_int32()
+    sizes = np.zeros(g.V, np.uint64)
+    capi.check(_L().vsgm_view_packing(device, g.V, capi.ptr(g.row_ptrs, C.c_uint64), capi.ptr(g.cols, C.c_uint32), capi.ptr(order, C.c_uint32),
+                                      capi.ptr(seq_offsets, C.c_uint64), len(seq_offsets) - 1, hop, cap, capi.ptr(bins, C.c_int32), C.byref(nb),
+                                      capi.ptr(sizes, C.c_uint64), g.V))
+    return bins, nb.value, sizes[:nb.value].copy()
+
+
 # -------------------------------------------------------------------- engine
 def view_compact(g):
     """Compact form of a full-V view: (ascending vertices with a non-empty row,

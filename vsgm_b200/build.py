@@ -1,4 +1,5 @@
-"""Build the native library in-tree: vsgm_b200/libvsgm_b200.so (+ the pm_pipeline driver).
+"""Build the native library in-tree: vsgm_b200/libvsgm_b200.so (+ the pm_pipeline driver
+and the view_tools driver).
 
     python -m vsgm_b200.build [--force]
 
@@ -18,11 +19,12 @@ INC = os.path.join(ROOT, "include")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "libvsgm_b200.so")
 DRIVER = os.path.join(PKG, "pm_pipeline")
+VIEW_TOOLS = os.path.join(PKG, "view_tools")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_SRCS = ["planner.cpp", "graph.cpp", "capi_host.cpp"]
-CUDA_SRCS = ["engine.cu", "mlp.cu"]
+CUDA_SRCS = ["engine.cu", "mlp.cu", "partition.cu"]
 
 
 def _newest(paths):
@@ -67,6 +69,9 @@ def build(force=False, verbose_ptxas=False):
     if os.path.exists(drv) and _stale(DRIVER, [drv, LIB] + hdrs, force):
         _run(["g++", "-std=c++17", "-O3", "-fopenmp", f"-I{INC}", drv, "-o", DRIVER, f"-L{PKG}", "-lvsgm_b200",
               "-Wl,-rpath,$ORIGIN"])
+    tools = os.path.join(CSRC, "view_tools.cpp")
+    if os.path.exists(tools) and _stale(VIEW_TOOLS, [tools, LIB] + hdrs, force):
+        _run(["g++", "-std=c++17", "-O3", f"-I{INC}", tools, "-o", VIEW_TOOLS, f"-L{PKG}", "-lvsgm_b200", "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

@@ -131,6 +131,10 @@ _SIGS = {
     "vsgm_random_pattern": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_uint64, _u64p, _P(C.c_int), _u8p]),
     "vsgm_view_materialize": (C.c_int, [C.c_uint64, _u64p, _u32p, _u32p, C.c_uint64, C.c_int, C.c_uint64, C.c_int,
                                         _u64p, _u32p, C.c_uint64, _u64p]),
+    "vsgm_features_1hop": (C.c_int, [C.c_int, C.c_uint64, _u64p, _u32p, _u64p, _u32p]),
+    "vsgm_kmeans": (C.c_int, [C.c_int, C.c_uint64, _u64p, _u32p, C.c_int, C.c_int, _i32p, C.c_int, C.c_int, _i32p, _P(C.c_int64), _i32p]),
+    "vsgm_view_packing": (C.c_int, [C.c_int, C.c_uint64, _u64p, _u32p, _u32p, _u64p, C.c_int, C.c_int, C.c_uint64, _i32p, _i32p, _u64p,
+                                    C.c_uint64]),
     "vsgm_create": (C.c_int, [C.c_int, C.c_uint64, _P(Plan), C.c_int, C.c_uint64, C.c_uint64, _P(C.c_void_p)]),
     "vsgm_transfer_view": (C.c_int, [C.c_void_p, _u64p, _u32p, C.c_uint64, _u32p, C.c_uint64]),
     "vsgm_bind_view_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_uint64]),

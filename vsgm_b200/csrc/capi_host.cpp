@@ -24,6 +24,8 @@ T* export_vec(const std::vector<T>& v) {
 }
 }  // namespace
 
+void vsgm::set_host_error(const std::string& msg) { g_err = msg; }
+
 extern "C" {
 
 const char* vsgm_last_error(void) { return g_err.c_str(); }

@@ -74,4 +74,8 @@ void degree_relabel(const Csr& g, bool ascending, int threads, std::vector<uint3
 // `seed` starting at *counter, which is advanced past the draws used.
 void random_pattern(int n_min, int n_max, double p, uint64_t seed, uint64_t* counter, int* n, uint8_t bits[7]);
 
+// Message returned by vsgm_last_error on this thread (for entry points defined
+// outside capi_host.cpp).
+void set_host_error(const std::string& msg);
+
 }  // namespace vsgm

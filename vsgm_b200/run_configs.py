@@ -15,6 +15,8 @@ c4  the learned planner on c3-distributed (pattern, view) pairs (seed 4): the
     network is trained by the library's MLP kernels on measured per-op work of
     candidate orders; held-out pairs report the work of the heuristic order and
     of the verified learned choice on an independent root sample.
+views  the view-bin chain (features, kmeans, view_packing) of C2 on the device,
+    timed and, with --reference, compared with the reference's own tools.
 c5  Chung-Lu, 65M vertices, ~1.8B edges, exponent 2.2, max degree 5000, seed 5
     (use --scale-down k for a 1/k-size graph of the same shape): -kc 3, -kc 4,
     -p 4 (house), whole graph as one view, plus the same totals over 4
@@ -134,11 +136,13 @@ def run_c3(args):
         lcounts = [[0] * len(views) for _ in plans]
         for (a, vi), c in zip(pair_list, got):
             lcounts[uniq[a][0]][vi] = c
-        learned = {"wall_ms": l_wall * 1e3, "device_ms": lst.ms, "level_pairs": int(lst.level_pairs), "tasks": int(lst.tasks),
+        learned = {"changed_pairs": [[int(keep[pi]), vi] for vi in range(len(views)) for pi, (_, took) in enumerate(chosen[vi]) if took],
+                   "wall_ms": l_wall * 1e3, "device_ms": lst.ms, "level_pairs": int(lst.level_pairs), "tasks": int(lst.tasks),
                    "orders_changed": sum(int(took) for row in chosen for _, took in row), "plan_s": t_plan, "train_s": t_train,
                    "counts": lcounts}
     # plain: the level-wise engine, one view after the other (uploads outside the timing)
     plain = [[0] * len(views) for _ in plans]
+    pair_ms = np.zeros((len(plans), len(views)))
     p_ms = p_wall = 0.0
     launches = 0
     with Engine(V, plans) as e:
@@ -154,7 +158,8 @@ def run_c3(args):
             for pi, p in enumerate(plans):
                 plain[pi][vi] = c[pi]
                 s = e.stats(pi)
-                p_ms += sum(s.op_ms[j] for j in range(p.n_ops))
+                pair_ms[pi, vi] = sum(s.op_ms[j] for j in range(p.n_ops))
+                p_ms += pair_ms[pi, vi]
                 launches += sum(s.op_launches[j] for j in range(p.n_ops))
     total = sum(sum(r) for r in plain)
     out = {"config": "c3", "views": [(g.V, g.E) for g in views], "patterns_run": len(keep),
@@ -163,6 +168,12 @@ def run_c3(args):
            "batched": {"device_ms": b_ms, "wall_ms": b_wall * 1e3, "tasks": int(tasks), "level_pairs": int(b_level)},
            "plain": {"device_ms": p_ms, "wall_ms": p_wall * 1e3, "launches": int(launches)},
            "speedup_wall": p_wall / b_wall if b_wall else None}
+    # where the plain engine's time goes: the heaviest (pattern, view) pairs
+    top = np.argsort(pair_ms, axis=None)[::-1][:16]
+    out["plain_top_pairs"] = [{"pattern": int(keep[i // len(views)]), "view": int(i % len(views)), "ms": float(pair_ms.flat[i]),
+                               "vertices": int(plans[i // len(views)].n_vertices), "edges": int(plans[i // len(views)].n_edges),
+                               "count": int(plain[i // len(views)][i % len(views)])} for i in top]
+    out["plain_top16_share"] = float(pair_ms.flat[top].sum() / max(pair_ms.sum(), 1e-9))
     if learned:
         out["learned_identical_counts"] = learned.pop("counts") == plain
         out["batched_learned"] = learned
@@ -268,9 +279,73 @@ def run_c5(args):
     return out
 
 
+def run_views(args):
+    """The view-bin chain of C2 on the device: features -h 1, kmeans -k 4 -i
+    --kmeans-iters -init 1, view_packing -h 2 at 40 GB and at 0.45 GB, on R-MAT 22
+    in the generator's ids; with --reference the reference's own tools (built in
+    oracle/_ref) run on the same files with all host threads, their outputs are
+    compared and both are timed.  The reference kmeans runs with -t 1 when
+    --reference-kmeans-t1 is given (its random start is then the same draw)."""
+    import os
+    import shutil
+    import subprocess
+    import tempfile
+
+    from . import features_1hop, kmeans, packing_order, reference_rand_starts, view_packing, write_csr_bin
+    g = gen_rmat(22, 16, *wl.RMAT_ABC, seed=2)
+    out = {"config": "views", "graph": f"R-MAT 22 ef 16 seed 2, V={g.V}, E={g.E}", "kmeans_iters": args.kmeans_iters}
+    t = time.perf_counter()
+    h = features_1hop(g)
+    out["features_ms"] = (time.perf_counter() - t) * 1e3
+    t = time.perf_counter()
+    part, sizes = kmeans(h, 4, args.kmeans_iters, starts=reference_rand_starts(4, 1))
+    out["kmeans_ms"] = (time.perf_counter() - t) * 1e3
+    out["cluster_sizes"] = sizes.tolist()
+    order, offs = packing_order(part, "1x4", 1)
+    for mem in (40, 0.45):
+        t = time.perf_counter()
+        bins, nb, _ = view_packing(g, order, offs, 2, mem)
+        out[f"packing_{mem}GB_ms"] = (time.perf_counter() - t) * 1e3
+        out[f"packing_{mem}GB_bins"] = nb
+    if args.reference:
+        ref = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref")
+        threads = str(os.cpu_count() or 1)
+        with tempfile.TemporaryDirectory() as d:
+            write_csr_bin(os.path.join(d, "g.bin"), g)
+
+            def timed(*cmd):
+                t0 = time.perf_counter()
+                r = subprocess.run(list(cmd), cwd=d, capture_output=True, text=True, timeout=3600)
+                if r.returncode != 0:
+                    raise RuntimeError(r.stderr[-500:])
+                return (time.perf_counter() - t0) * 1e3
+
+            out["reference_threads"] = int(threads)
+            out["reference_features_ms"] = timed(os.path.join(ref, "features"), "-f", "g.bin", "-h", "1", "-t", threads)
+            kt = "1" if args.reference_kmeans_t1 else threads
+            out["reference_kmeans_threads"] = int(kt)
+            out["reference_kmeans_ms"] = timed(os.path.join(ref, "kmeans"), "-f", "g.bin.1hop.bin", "-k", "4", "-i", str(args.kmeans_iters), "-t", kt,
+                                               "-init", "1")
+            want = np.loadtxt(os.path.join(d, "g.bin.1hop.bin.kmeans.4"), dtype=np.int32)
+            if kt == "1":
+                out["kmeans_equal_reference"] = bool(np.array_equal(want, part))
+            shutil.copy(os.path.join(d, "g.bin.1hop.bin.kmeans.4"), os.path.join(d, "g.bin.kmeans.1x4"))
+            r_order, r_offs = packing_order(want, "1x4", 1)
+            for mem in (40, 0.45):
+                out[f"reference_packing_{mem}GB_ms"] = timed(os.path.join(ref, "view_packing"), "-gf", "g.bin", "-pf", "g.bin.kmeans.1x4", "-h", "2",
+                                                             "-m", str(mem), "-t", "1", "-s", "1")
+                wb = np.loadtxt(os.path.join(d, "g.bin.2.hop.vbmap"), dtype=np.int32)
+                bins, nb, _ = view_packing(g, r_order, r_offs, 2, mem)
+                out[f"packing_{mem}GB_equal_reference"] = bool(int(wb[0]) == nb and np.array_equal(wb[1:], bins))
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("config", choices=["c1", "c3", "c4", "c5"])
+    ap.add_argument("config", choices=["c1", "c3", "c4", "c5", "views"])
+    ap.add_argument("--kmeans-iters", type=int, default=10, help="views: k-means iterations")
+    ap.add_argument("--reference", action="store_true", help="views: also run and compare the reference's tools from oracle/_ref")
+    ap.add_argument("--reference-kmeans-t1", action="store_true", help="views: run the reference kmeans with -t 1 (same random start)")
     ap.add_argument("--e-max", type=float, default=None)
     ap.add_argument("--max-work", type=float, default=5e9)
     ap.add_argument("--views", type=int, default=8)
@@ -283,7 +358,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.e_max is None:
         args.e_max = {"c3": 1e6, "c4": 2e5}.get(args.config, 1e7)
-    out = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5}[args.config](args)
+    out = {"c1": run_c1, "c3": run_c3, "c4": run_c4, "c5": run_c5, "views": run_views}[args.config](args)
     print(json.dumps(out), flush=True)
     return 0
 
