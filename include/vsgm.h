@@ -325,7 +325,11 @@ int vsgm_mlp_destroy(vsgm_mlp* m);
  *   groups sharing the whole GPU with L2-resident counters (0: every root);
  *   "c4_window" (default 0): heavy roots with fewer than 65536 lower neighbours count
  *   the wedges ending in the 393,216 ids just below them in the distributed shared
- *   memory of a 4-block cluster, the rest in the groups;
+ *   memory of a 4-block cluster, the rest in the groups (measured slower on R-MAT 22);
+ *   "c4_balance" (default 0): a heavy group's wedge launch splits its centres'
+ *   adjacency entries evenly over the warps instead of giving each warp whole
+ *   centres (faster per launch alone, slower in the two-stream group pipeline on
+ *   R-MAT 22);
  *   "c4_hash" (default 1): the other roots keep their counters in a shared-memory
  *   hash table (a warp per root up to 768 wedges, a block up to 12288; beyond, and
  *   with 0, one block per root with dense counters in HBM);

@@ -92,7 +92,7 @@ def test_c2_bench_operators_on_hub_roots(vs, orc, rmat22):
     assert min(want) > 0
     # the defaults, then the alternatives the knobs select
     for knobs in ({}, {"clique_bits": 0}, {"clique_bits": 0, "tail_merge": 1}, {"clique_bits": 0, "fuse_tail": 0},
-                  {"clique_bits": 0, "lane_slice": 0}, {"c4_heavy": 0}, {"c4_heavy": 1 << 40}, {"c4_heavy": 1 << 16, "c4_hash": 0}, {"c4_window": 1}, {"edge_triangles": 0},
+                  {"clique_bits": 0, "lane_slice": 0}, {"c4_heavy": 0}, {"c4_heavy": 1 << 40}, {"c4_heavy": 1 << 16, "c4_hash": 0}, {"c4_window": 1}, {"c4_balance": 1}, {"c4_window": 1, "c4_balance": 1}, {"edge_triangles": 0},
                   {"edge_triangles": 0, "set_reuse": 0}):
         with vs.Engine(g.V, plans) as e:
             for name, value in knobs.items():

@@ -356,16 +356,18 @@ def test_four_cycle_aggregation_equals_plan(vs, orc, graphs):
         want = orc.count(p, g)
         # c4_heavy 0: every root through the group kernels; 2^40: none; c4_hash 0:
         # light roots through dense counters in HBM instead of shared-memory tables
-        for agg, heavy, hashed, window in ((1, 1 << 40, 1, 0), (1, 1 << 40, 0, 0), (1, 0, 1, 0), (1, 0, 1, 1), (1, 64, 1, 1), (1, 64, 0, 0),
-                                           (1, 12289, 1, 0), (0, 0, 1, 0)):
+        # c4_balance 1: heavy groups split by adjacency entry instead of by centre
+        for agg, heavy, hashed, window, bal in ((1, 1 << 40, 1, 0, 1), (1, 1 << 40, 0, 0, 1), (1, 0, 1, 0, 1), (1, 0, 1, 0, 0), (1, 0, 1, 1, 1),
+                                                (1, 64, 1, 1, 1), (1, 64, 0, 0, 1), (1, 64, 0, 0, 0), (1, 12289, 1, 0, 1), (0, 0, 1, 0, 1)):
             with vs.Engine(g.V, [p]) as e:
                 e.set_option("c4_aggregate", agg)
                 e.set_option("c4_heavy", heavy)
                 e.set_option("c4_hash", hashed)
                 e.set_option("c4_window", window)
+                e.set_option("c4_balance", bal)
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
                 e.match()
-                assert e.counts() == [want], (agg, heavy, hashed, window)
+                assert e.counts() == [want], (agg, heavy, hashed, window, bal)
     # views: per-view attribution differs, totals do not
     g = graphs["rmat8"]
     bins = (np.arange(g.V) % 3).astype(np.int32)
@@ -534,10 +536,30 @@ def test_four_cycle_wide_and_packed_counters(vs, orc):
     g, _ = vs.degree_relabel(vs.Graph(rp, np.array([x for r in rows for x in sorted(r)], dtype=np.uint32)))
     want = orc.c4_by_largest_wedges(g)
     for heavy in (0, 1 << 10, 12289):
-        for window in (0, 1):
+        for window, bal in ((0, 1), (1, 1), (0, 0)):
             with vs.Engine(g.V, [vs.plan_pattern(1)]) as e:
                 e.set_option("c4_heavy", heavy)
                 e.set_option("c4_window", window)
+                e.set_option("c4_balance", bal)
                 e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
                 e.match()
-                assert e.counts() == [want], (heavy, window)
+                assert e.counts() == [want], (heavy, window, bal)
+
+
+def test_isomorphic_queries_count_alike(vs, orc, graphs):
+    """The batched runs count one pattern per isomorphism class of the batch: on a
+    view whose every vertex is a source, relabelled copies of a pattern (different
+    plans, different roots) have the same exact count, and it is the oracle's."""
+    from vsgm_b200 import workloads as wl
+    pats = [p for p in wl.random_patterns(64, seed=3) if p.n_vertices <= 5]
+    reps, cls = vs.query_classes(pats)
+    assert len(reps) < len(pats)
+    g = graphs["rmat7"]
+    with vs.Engine(g.V, pats) as e:
+        e.transfer_view(g, np.arange(g.V, dtype=np.uint32))
+        e.match()
+        got = e.counts()
+    for i, p in enumerate(pats):
+        assert got[i] == got[reps[cls[i]]], i
+    for r in reps:
+        assert got[r] == orc.count(pats[r], g), r

@@ -156,6 +156,7 @@ struct vsgm_engine {
     uint64_t c4_heavy = kC4HashBlockMaxW + 1;  // 4-cycle roots with at least this many wedges use the L2-resident group kernels
     bool c4_hash = true;             // 4-cycle light roots: counters in a shared-memory hash table
     bool c4_window = false;          // 4-cycle heavy roots: the ids just below the root counted in cluster shared memory
+    bool c4_balance = false;         // 4-cycle heavy groups: work split by adjacency entries instead of by wedge centre
     uint32_t walk_ratio = 8;         // fused tail: walk N(c) unless it is this many times longer than the slice
     uint32_t lane_slice = kLaneSlice;  // fused tail: longest slice a lane handles alone
     bool tail_merge = false;           // fused tail: heavy children by a merge-path split over the lanes
@@ -944,6 +945,7 @@ struct vsgm_engine {
       const int Gw = (int)std::max<uint64_t>(1, std::min<uint64_t>(kC4Group, buf / (stride_w * 4)));
       std::vector<C4Group> groups;
       std::vector<uint8_t> packed;
+      uint64_t n_centres = 0;  // centres of all groups, in group order (the balanced kernel's prefix)
       auto make_groups = [&](const std::vector<uint32_t>& r, const std::vector<uint64_t>& c, const std::vector<uint32_t>& lim, int G, bool pk) {
         for (uint64_t k = 0; k < r.size(); k += G) {
           C4Group g;
@@ -954,6 +956,8 @@ struct vsgm_engine {
             g.lim[i] = lim[k + i];
             g.vbeg[i + 1] = g.vbeg[i] + c[k + i];
           }
+          g.cbase = n_centres;
+          n_centres += g.vbeg[g.n];
           groups.push_back(g);
           packed.push_back(pk ? 1 : 0);
         }
@@ -967,6 +971,16 @@ struct vsgm_engine {
         CK(cudaMemcpyAsync(d_groups, groups.data(), groups.size() * sizeof(C4Group), cudaMemcpyHostToDevice, stream));
         CK(cudaMemsetAsync(Lbuf[0], 0, words * sizeof(uint32_t), stream));
         CK(cudaMemsetAsync(Lbuf[1], 0, words * sizeof(uint32_t), stream));
+        uint64_t* P = nullptr;
+        if (cur.c4_balance) {
+          // prefix of every centre's row length, the entry space the balanced kernel splits
+          uint32_t* deg = arena.take_n<uint32_t>(n_centres + 1, "4-cycle centre degrees");
+          P = arena.take_n<uint64_t>(n_centres + 1, "4-cycle centre prefix");
+          k_c4_centre_degrees<<<(unsigned)groups.size(), 256, 0, stream>>>(d_rp, d_ci, d_groups, deg);
+          CK(cudaGetLastError());
+          scan(deg, true, n_centres, P);
+          launches += 1;
+        }
         CK(cudaEventRecord(ev_fork, stream));
         CK(cudaStreamWaitEvent(aux_stream, ev_fork, 0));
         const unsigned gw = (unsigned)sms * 8, gs = (unsigned)sms * 4;
@@ -974,10 +988,16 @@ struct vsgm_engine {
           cudaStream_t st2 = (i & 1) ? aux_stream : stream;  // group i uses buffer i % 2 on stream i % 2
           uint32_t* L = Lbuf[i & 1];
           if (packed[i]) {
-            k_c4_group_wedges<true><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_p);
+            if (P)
+              k_c4_group_wedges_bal<true><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, P, L, stride_p);
+            else
+              k_c4_group_wedges<true><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_p);
             k_c4_group_sum<true><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_p, d_total);
           } else {
-            k_c4_group_wedges<false><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_w);
+            if (P)
+              k_c4_group_wedges_bal<false><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, P, L, stride_w);
+            else
+              k_c4_group_wedges<false><<<gw, 256, 0, st2>>>(d_rp, d_ci, d_groups + i, L, stride_w);
             k_c4_group_sum<false><<<gs, 256, 0, st2>>>(d_groups + i, L, stride_w, d_total);
           }
         }
@@ -1952,6 +1972,10 @@ int vsgm_set_plan_option(vsgm_engine* e, int plan, const char* name, int64_t val
   if (n == "walk_ratio") {
     if (value < 0 || value > 65535) return engine_fail(e, VSGM_EINVAL, "walk_ratio must be 0..65535");
     for (int k = lo; k < hi; k++) e->knobs[k].walk_ratio = (uint32_t)value;
+    return VSGM_OK;
+  }
+  if (n == "c4_balance") {
+    for (int k = lo; k < hi; k++) e->knobs[k].c4_balance = value != 0;
     return VSGM_OK;
   }
   if (n == "c4_window") {

@@ -1074,6 +1074,7 @@ struct C4Group {
   uint32_t root[kC4Group];
   uint32_t lim[kC4Group];            // wedge ends w < lim are counted here (the root itself, or the start of its window)
   uint64_t vbeg[kC4Group + 1];       // prefix of the wedge centres (neighbours below the root) per root
+  uint64_t cbase;                    // index of the group's first centre in the centre-degree prefix (balanced kernel)
 };
 
 
@@ -1164,6 +1165,89 @@ __global__ void __launch_bounds__(256) k_c4_group_wedges(const uint64_t* __restr
       }
       if (__any_sync(kFull, w >= lim)) break;
     }
+  }
+}
+
+// Row lengths of every group's wedge centres, in group order (centre k of root
+// slot i of group g at grp[g].cbase + vbeg[i] + k): the input of the prefix that
+// the balanced kernel splits its work by.  One block per group.
+__global__ void k_c4_centre_degrees(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci, const C4Group* __restrict__ grp,
+                                    uint32_t* __restrict__ deg) {
+  const C4Group& G = grp[blockIdx.x];
+  for (uint32_t i = 0; i < G.n; i++) {
+    const uint64_t ua = __ldg(rp + G.root[i]), nc = G.vbeg[i + 1] - G.vbeg[i];
+    for (uint64_t k = threadIdx.x; k < nc; k += blockDim.x) {
+      const uint32_t v = __ldg(ci + ua + k);
+      deg[G.cbase + G.vbeg[i] + k] = (uint32_t)(__ldg(rp + v + 1) - __ldg(rp + v));
+    }
+  }
+}
+
+// k_c4_group_wedges with the work split by adjacency entries instead of by centre:
+// P is the exclusive prefix of the centres' row lengths (k_c4_centre_degrees), and
+// warp w of the grid takes the group's entries [w*share, (w+1)*share) - one search
+// for its first centre, then a walk across centres - so a hub centre's long row is
+// shared by many warps and no warp waits on another's tail.  A centre's walk stops
+// at the first entry >= lim (rows are sorted); two strides are loaded per step.
+template <bool kPacked>
+__global__ void __launch_bounds__(256) k_c4_group_wedges_bal(const uint64_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                                             const C4Group* __restrict__ grp, const uint64_t* __restrict__ P,
+                                                             uint32_t* __restrict__ L, uint64_t stride) {
+  const C4Group& G = *grp;
+  const uint64_t nc = G.vbeg[G.n];
+  const uint64_t* Pg = P + G.cbase;
+  const uint64_t E0 = Pg[0], total = Pg[nc] - E0;
+  const uint64_t warps = (uint64_t)gridDim.x * blockDim.x / kWarp;
+  const uint64_t wid = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const unsigned lane = lane_id();
+  const uint64_t share = (total + warps - 1) / warps;
+  const uint64_t s = wid * share, e = min(total, s + share);
+  if (s >= e) return;
+  // the centre holding entry s: the last c with Pg[c] - E0 <= s (Pg is non-decreasing)
+  uint64_t c = 0;
+  if (lane == 0) {
+    uint64_t lo = 0, hi = nc;  // invariant: Pg[lo] - E0 <= s < Pg[hi] - E0
+    while (hi - lo > 1) {
+      const uint64_t mid = (lo + hi) / 2;
+      if (Pg[mid] - E0 <= s)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    c = lo;
+  }
+  c = __shfl_sync(kFull, c, 0);
+  uint32_t g = 0;
+  while (g + 1 < G.n && c >= G.vbeg[g + 1]) g++;
+  uint64_t pos = s;
+  while (pos < e && c < nc) {
+    const uint64_t rb = Pg[c] - E0, re = Pg[c + 1] - E0;  // this centre's entries
+    const uint32_t u = G.root[g], lim = G.lim[g];
+    const uint32_t v = __ldg(ci + __ldg(rp + u) + (c - G.vbeg[g]));
+    uint32_t* Lg = L + (uint64_t)g * stride;
+    const uint64_t row = __ldg(rp + v);
+    const uint64_t j0 = row + (pos - rb), jend = row + (min(e, re) - rb);
+    for (uint64_t jb = j0; jb < jend; jb += 2 * kWarp) {
+      const uint64_t j1 = jb + lane, j2 = j1 + kWarp;
+      const uint32_t w1 = j1 < jend ? __ldg(ci + j1) : lim;
+      const uint32_t w2 = j2 < jend ? __ldg(ci + j2) : lim;
+      if (w1 < lim) {
+        if (kPacked)
+          atomicAdd(Lg + (w1 >> 1), (w1 & 1u) ? 0x10000u : 1u);
+        else
+          atomicAdd(Lg + w1, 1u);
+      }
+      if (w2 < lim) {
+        if (kPacked)
+          atomicAdd(Lg + (w2 >> 1), (w2 & 1u) ? 0x10000u : 1u);
+        else
+          atomicAdd(Lg + w2, 1u);
+      }
+      if (__any_sync(kFull, w2 >= lim)) break;  // w2 >= w1 in every lane that loaded both
+    }
+    pos = re;
+    c++;
+    while (g + 1 < G.n && c >= G.vbeg[g + 1]) g++;
   }
 }
 
