@@ -122,3 +122,32 @@ def test_autotune_view_classes():
     c = TuneCache()
     c.put(b"plan", view_class(a), {"fuse_tail": 0})
     assert c.get(b"plan", view_class(b)) == {"fuse_tail": 0} and c.get(b"other", view_class(b)) is None
+
+
+def test_query_classes_group_isomorphic_patterns(vs):
+    """Relabelled copies of a pattern fall into one class, different patterns into
+    different classes (the batched runs count each class once)."""
+    import itertools
+    import random
+
+    def bits_of(n, edges):
+        b = [0] * 7
+        for i, j in edges:
+            b[i] |= 1 << j
+            b[j] |= 1 << i
+        return b
+
+    rng = random.Random(5)
+    shapes = {"house": (5, [(0, 1), (1, 2), (2, 3), (3, 4), (4, 0), (1, 4)]), "c5": (5, [(0, 1), (1, 2), (2, 3), (3, 4), (4, 0)]),
+              "path4": (4, [(0, 1), (1, 2), (2, 3)]), "star4": (4, [(0, 1), (0, 2), (0, 3)]), "tri": (3, [(0, 1), (1, 2), (0, 2)])}
+    plans, truth = [], []
+    for name, (n, edges) in shapes.items():
+        for _ in range(3):
+            perm = list(range(n))
+            rng.shuffle(perm)
+            plans.append(vs.plan_query_bits(n, bits_of(n, [(perm[i], perm[j]) for i, j in edges])))
+            truth.append(name)
+    reps, cls = vs.query_classes(plans)
+    assert len(reps) == len(shapes)
+    for a, b in itertools.combinations(range(len(plans)), 2):
+        assert (cls[a] == cls[b]) == (truth[a] == truth[b])

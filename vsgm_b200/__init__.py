@@ -438,6 +438,37 @@ class Engine:
             pass
 
 
+def canonical_pattern(plan):
+    """Canonical form of a planned pattern's graph: the largest upper-triangle
+    adjacency bit string over all relabellings of its vertices (n <= 7, so at most
+    5040 of them).  Two patterns are isomorphic iff their forms are equal."""
+    import itertools
+    n = plan.n_vertices
+    A = [[(plan.adj[i] >> j) & 1 for j in range(n)] for i in range(n)]
+    pairs = [(i, j) for i in range(n) for j in range(i + 1, n)]
+    best = max(tuple(A[p[i]][p[j]] for i, j in pairs) for p in itertools.permutations(range(n)))
+    return n, best
+
+
+def query_classes(plans):
+    """Isomorphism classes of a batch of queries: (representative plan index per
+    class, class of every plan).  A batch often holds the same pattern under
+    different vertex labellings (random queries of 3-6 vertices fall into few
+    classes); over a view whose every vertex is a source, isomorphic patterns have
+    the same exact count whatever their plans, so a batch needs to count each class
+    once.  (With views that split the sources, per-view counts of isomorphic
+    patterns can differ - their plans may root a match at different pattern
+    vertices - and only the totals over all views agree.)"""
+    reps, cls, seen = [], [], {}
+    for i, p in enumerate(plans):
+        key = canonical_pattern(p)
+        if key not in seen:
+            seen[key] = len(reps)
+            reps.append(i)
+        cls.append(seen[key])
+    return reps, cls
+
+
 def count_graph(g, plans, sources=None, device=0, hbm_budget_bytes=0, views=None, hop=None):
     """Exact counts of every plan over g (all vertices as sources, one view), or
     over a list of per-view source arrays, each materialised with the plans' hop."""

@@ -9,8 +9,11 @@ c3  64 random connected patterns (3-6 vertices, p = 0.5, seed 3) x 16 Chung-Lu
     the configuration's 1e7 with --e-max 1e7), max degree 1e4, seed 3): the
     persistent batched (hybrid) run and, with --learned, the batched run over the
     learned planner's orders, against the plain level-wise engine with the
-    heuristic order view after view, at identical counts.  Patterns whose sampled
-    work exceeds --max-work on some view are left out and listed.
+    heuristic order view after view, at identical counts.  The batched runs count
+    each isomorphism class of the batch once (every view holds all its vertices as
+    sources, so isomorphic patterns have equal counts; --no-dedup counts every
+    pattern).  Patterns whose sampled work exceeds --max-work on some view are left
+    out and listed.
 c4  the learned planner on c3-distributed (pattern, view) pairs (seed 4): the
     network is trained by the library's MLP kernels on measured per-op work of
     candidate orders; held-out pairs report the work of the heuristic order and
@@ -33,7 +36,7 @@ import time
 
 import numpy as np
 
-from . import Engine, Graph, degree_relabel, gen_rmat, plan_clique, plan_pattern
+from . import Engine, Graph, degree_relabel, gen_rmat, plan_clique, plan_pattern, query_classes
 from . import planner as lp
 from . import workloads as wl
 
@@ -96,35 +99,43 @@ def run_c3(args):
     keep = [i for i in range(len(pats)) if not ovf[i].any() and work[i].max() < args.max_work]
     plans = [pats[i] for i in keep]
     V = max(g.V for g in views)
-    # batched: every (pattern, view) pair in one persistent (hybrid) run
-    with Engine(V, plans) as e:
+    # the batch's isomorphism classes: every view holds all its vertices as sources,
+    # so one count per class and view serves every pattern of the class
+    if args.no_dedup:
+        reps, cls = list(range(len(plans))), list(range(len(plans)))
+    else:
+        reps, cls = query_classes(plans)
+    rplans = [plans[i] for i in reps]
+    # batched: every (class representative, view) pair in one persistent (hybrid) run
+    with Engine(V, rplans) as e:
         ids = [e.add_view(g) for g in views]
         e.set_profiling(True)
         e.run_batched(ids)  # warm-up
         t = time.perf_counter()
-        batched = e.run_batched(ids)
+        rb = e.run_batched(ids)
         b_wall = time.perf_counter() - t
         st = e.batch_stats()
         b_ms, tasks, b_level = st.ms, st.tasks, st.level_pairs
+    batched = [rb[cls[pi]] for pi in range(len(plans))]
     learned = None
     if args.learned:
-        # batched + learned: the planner proposes orders per (pattern, view), the
+        # batched + learned: the planner proposes orders per (class, view), the
         # level-wise engine times them on a root sample of that view, then one
         # hybrid run over the chosen plans
         model, t_train = _train_planner(args)
         sampler = lp.Sampler(views, roots_per_view=256, seed=1, step_budget=500_000)
         t = time.perf_counter()
-        chosen = [model.choose_timed_many(plans, sampler, vi, k=4) for vi in range(len(views))]
+        chosen = [model.choose_timed_many(rplans, sampler, vi, k=4) for vi in range(len(views))]
         t_plan = time.perf_counter() - t
         model.close()
         uniq, pair_list = [], []
         for vi in range(len(views)):
-            for pi, (order, _) in enumerate(chosen[vi]):
-                key = (pi, tuple(order))
+            for ri, (order, _) in enumerate(chosen[vi]):
+                key = (ri, tuple(order))
                 if key not in uniq:
                     uniq.append(key)
                 pair_list.append((uniq.index(key), vi))
-        lplans = [lp.plan_reorder(plans[pi], o) for pi, o in uniq]
+        lplans = [lp.plan_reorder(rplans[ri], o) for ri, o in uniq]
         with Engine(V, lplans) as e:
             ids = [e.add_view(g) for g in views]
             e.set_profiling(True)
@@ -133,10 +144,11 @@ def run_c3(args):
             got = e.run_pairs([(a, ids[b]) for a, b in pair_list])
             l_wall = time.perf_counter() - t
             lst = e.batch_stats()
-        lcounts = [[0] * len(views) for _ in plans]
+        rcounts = [[0] * len(views) for _ in rplans]
         for (a, vi), c in zip(pair_list, got):
-            lcounts[uniq[a][0]][vi] = c
-        learned = {"changed_pairs": [[int(keep[pi]), vi] for vi in range(len(views)) for pi, (_, took) in enumerate(chosen[vi]) if took],
+            rcounts[uniq[a][0]][vi] = c
+        lcounts = [rcounts[cls[pi]] for pi in range(len(plans))]
+        learned = {"changed_pairs": [[int(keep[reps[ri]]), vi] for vi in range(len(views)) for ri, (_, took) in enumerate(chosen[vi]) if took],
                    "wall_ms": l_wall * 1e3, "device_ms": lst.ms, "level_pairs": int(lst.level_pairs), "tasks": int(lst.tasks),
                    "orders_changed": sum(int(took) for row in chosen for _, took in row), "plan_s": t_plan, "train_s": t_train,
                    "counts": lcounts}
@@ -162,7 +174,8 @@ def run_c3(args):
                 p_ms += pair_ms[pi, vi]
                 launches += sum(s.op_launches[j] for j in range(p.n_ops))
     total = sum(sum(r) for r in plain)
-    out = {"config": "c3", "views": [(g.V, g.E) for g in views], "patterns_run": len(keep),
+    out = {"config": "c3", "views": [(g.V, g.E) for g in views], "patterns_run": len(keep), "pattern_classes": len(reps),
+           "dedup": not args.no_dedup,
            "patterns_left_out": [i for i in range(len(pats)) if i not in keep],
            "identical_counts": [list(map(int, r)) for r in batched] == plain, "matches": int(total),
            "batched": {"device_ms": b_ms, "wall_ms": b_wall * 1e3, "tasks": int(tasks), "level_pairs": int(b_level)},
@@ -353,6 +366,7 @@ def main(argv=None):
     ap.add_argument("--scale-down", type=int, default=1)
     ap.add_argument("--house-stride", type=int, default=1, help="c5: count the house on every k-th root only")
     ap.add_argument("--learned", action="store_true", help="c3: also run batched + learned orders")
+    ap.add_argument("--no-dedup", action="store_true", help="c3: batched runs count every pattern, not one per isomorphism class")
     ap.add_argument("--model", default=None, help="c3 --learned: planner parameters (.npy from c4 --save)")
     ap.add_argument("--save", default=None, help="c4: write the trained planner's parameters here")
     args = ap.parse_args(argv)
