@@ -41,6 +41,14 @@ WORKLOAD = {"workload": "rmat22_ef16_seed2_kc4_p1_p2", "graph": "R-MAT scale 22,
             "relabel": "degree-ascending ids (exact counts are invariant to relabelling)"}
 
 
+# DRAM bytes per step of the dominant op, from one ncu capture of the same bench
+# command (the launch list of one step kept under profiles/: cold-cache
+# dram__bytes_read.sum + dram__bytes_write.sum of the 4-cycle operator's kernels,
+# its heavy-root groups scaled from the 288 captured to all 5,940).  Only for the
+# workload it was taken on.
+MEASURED_TRAFFIC = {("rmat22_ef16_seed2_kc4_p1_p2", "-p 1"): 3.5e11}
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -331,7 +339,9 @@ def main():
     peak, peak_kind = load_peaks()
     achieved = (dom_bytes / (dom_ms / 1e3)) / 1e9 if dom_ms > 0 and dom_bytes > 0 else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "traffic": None, "kernel": f"plan {dom_plan} op {dom_op} ({vs.capi.OP_NAMES[plans[dom_plan].op_type[dom_op]]})",
+                "traffic": MEASURED_TRAFFIC.get((WORKLOAD["workload"], WORKLOAD["queries"][dom_plan])) if world == 1 else None,
+                "traffic_source": "ncu launch list of one step (profiles/), bytes per step of the op",
+                "kernel": f"plan {dom_plan} op {dom_op} ({vs.capi.OP_NAMES[plans[dom_plan].op_type[dom_op]]})",
                 "kernel_ms_per_step": dom_ms, "peak_kind": peak_kind, "timed_in": "one profiled pass after the timed steps"}
     per_query = []
     for pi, p in enumerate(plans):
