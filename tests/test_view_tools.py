@@ -90,3 +90,17 @@ def test_packing_order_follows_the_partition_suffix(vs):
     np.testing.assert_array_equal(offs, [0, 4, 8])
     with pytest.raises(ValueError):
         vs.packing_order(part, "4", 1)
+
+
+def test_view_tools_driver_refuses_unsupported_forms(vs, tmp_path):
+    """The drop-in driver stops with exit code 2 and a message, before touching a
+    GPU, for the forms it does not build: features beyond -h 1, kmeans -init 0
+    (the reference seeds it from the clock) and multi-level -k, view_packing -s > 1."""
+    from vsgm_b200 import build
+    cases = [["features", "-f", "g.bin", "-h", "2"], ["kmeans", "-f", "g.bin", "-k", "4", "-init", "0"],
+             ["kmeans", "-f", "g.bin", "-k", "2^3", "-init", "1"], ["kmeans", "-f", "g.bin", "-k", "4x4", "-init", "1"],
+             ["view_packing", "-gf", "g.bin", "-pf", "g.bin.kmeans.4", "-s", "2"], ["no_such_tool"]]
+    for args in cases:
+        r = subprocess.run([build.VIEW_TOOLS, *args], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+        assert r.returncode == 2, (args, r.returncode, r.stderr)
+        assert "view_tools" in r.stderr
