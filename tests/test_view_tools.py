@@ -104,3 +104,44 @@ def test_view_tools_driver_refuses_unsupported_forms(vs, tmp_path):
         r = subprocess.run([build.VIEW_TOOLS, *args], cwd=tmp_path, capture_output=True, text=True, timeout=60)
         assert r.returncode == 2, (args, r.returncode, r.stderr)
         assert "view_tools" in r.stderr
+
+
+def test_view_tool_entry_points_reject_bad_arguments(vs):
+    """Argument checks run on the host before any device work (no GPU needed): a
+    cluster count out of range, a start outside [0, K), an order that is not a
+    permutation, sequences that do not cover the vertices, an unsupported hop."""
+    import ctypes as C
+    L = vs.capi.lib()
+    g = vs.gen_rmat(6, 4, seed=3)
+    rp, ci = vs.capi.ptr(g.row_ptrs, C.c_uint64), vs.capi.ptr(g.cols, C.c_uint32)
+    assign = np.zeros(g.V, np.int32)
+    sizes = np.zeros(200, np.int64)
+    n = C.c_int32()
+
+    def km(k, starts):
+        st = np.asarray(starts, np.int32)
+        return L.vsgm_kmeans(0, g.V, rp, ci, k, 3, vs.capi.ptr(st, C.c_int32), len(st), 0, vs.capi.ptr(assign, C.c_int32),
+                             sizes.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(n))
+
+    assert km(0, [0]) == -1
+    assert km(129, [0]) == -1
+    assert km(4, [4]) == -1 and b"start" in L.vsgm_last_error()
+    assert km(4, [-1]) == -1
+
+    bins = np.zeros(g.V, np.int32)
+    nb = C.c_int32()
+
+    def pack(order, offs, hop=2):
+        order = np.asarray(order, np.uint32)
+        offs = np.asarray(offs, np.uint64)
+        return L.vsgm_view_packing(0, g.V, rp, ci, vs.capi.ptr(order, C.c_uint32), vs.capi.ptr(offs, C.c_uint64), len(offs) - 1, hop, 10**6,
+                                   vs.capi.ptr(bins, C.c_int32), C.byref(nb), None, 0)
+
+    ident = np.arange(g.V)
+    assert pack(np.zeros(g.V), [0, g.V]) == -1 and b"every vertex exactly once" in L.vsgm_last_error()
+    assert pack(ident, [0, g.V - 1]) == -1
+    assert pack(ident, [0, g.V // 2 + 1, g.V // 2, g.V]) == -1 and b"must not decrease" in L.vsgm_last_error()
+    assert pack(ident, [0, g.V], hop=4) == -1
+    out_rp = np.zeros(g.V + 1, np.uint64)
+    out_ci = np.zeros(g.E + g.V, np.uint32)
+    assert L.vsgm_features_1hop(0, 0, rp, ci, vs.capi.ptr(out_rp, C.c_uint64), vs.capi.ptr(out_ci, C.c_uint32)) == -1
