@@ -189,3 +189,33 @@ def degree_relabel(g, threads=0):
     rp, ci = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
     lib().oracle_degree_relabel(C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32), threads, C.byref(rp), C.byref(ci))
     return _take(rp, ci, g.V)
+
+
+def kmeans(g, k, iters, starts, reorder=False):
+    """Restated reference kmeans -init 1 (oracle_tools.cc): the cluster of every
+    vertex after `iters` rounds from the random start `starts` (one draw per
+    reference thread), empty clusters removed."""
+    starts = np.ascontiguousarray(starts, dtype=np.int32)
+    out = np.zeros(g.V, np.int32)
+    n = C.c_int32()
+    rc = lib().oracle_kmeans(C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32), int(k), int(iters), _p(starts, C.c_int32),
+                             len(starts), 1 if reorder else 0, _p(out, C.c_int32), C.byref(n))
+    if rc != 0:
+        raise ValueError("oracle_kmeans: bad arguments")
+    return out
+
+
+def view_packing(g, order, seq_offsets, hop, cap):
+    """Restated reference view_packing -s 1 (oracle_tools.cc): (bin of every vertex,
+    number of bins, row entries per bin) for bins of at most `cap` row entries."""
+    order = np.ascontiguousarray(order, dtype=np.uint32)
+    offs = np.ascontiguousarray(seq_offsets, dtype=np.uint64)
+    bins = np.zeros(g.V, np.int32)
+    sizes = np.zeros(max(g.V, 1), np.uint64)
+    nb = C.c_int32()
+    rc = lib().oracle_view_packing(C.c_uint64(g.V), _p(g.row_ptrs, C.c_uint64), _p(g.cols, C.c_uint32), _p(order, C.c_uint32),
+                                   _p(offs, C.c_uint64), len(offs) - 1, int(hop), C.c_uint64(int(cap)), _p(bins, C.c_int32), C.byref(nb),
+                                   _p(sizes, C.c_uint64))
+    if rc == -2:
+        raise ValueError("a source's view alone exceeds the bin size")
+    return bins, nb.value, sizes[:nb.value].copy()

@@ -43,6 +43,10 @@
  * 6. oracle_gen_rmat / oracle_degree_relabel: the benchmark's synthetic input
  *    (R-MAT graph, ids ascending with degree), so that the timed CPU baseline
  *    needs nothing from the product library.
+ * 7. oracle_tools.cc (same library): the reference's offline view-bin tools
+ *    restated, kmeans -init 1 and view_packing -s 1; pinned to the reference
+ *    tools' own outputs (tests/golden/ref_view_tools.npz and the binaries built in
+ *    oracle/_ref, tests/test_view_tools.py).
  *
  * Parity: the reference's matching path cannot be built here (its moderngpu and
  * MPMCQueue submodules are not vendored and it needs a GPU), and the reference

@@ -145,3 +145,63 @@ def test_view_tool_entry_points_reject_bad_arguments(vs):
     out_rp = np.zeros(g.V + 1, np.uint64)
     out_ci = np.zeros(g.E + g.V, np.uint32)
     assert L.vsgm_features_1hop(0, 0, rp, ci, vs.capi.ptr(out_rp, C.c_uint64), vs.capi.ptr(out_ci, C.c_uint32)) == -1
+
+
+def test_oracle_restatement_reproduces_the_reference_fixtures(vs, gold):
+    """The oracle's restatement of kmeans and view_packing (oracle/oracle_tools.cc)
+    gives the reference tools' own outputs on every fixture case."""
+    import oracle
+    for name in ["rmat", "chunglu"]:
+        h = vs.Graph(gold[f"{name}_1hop_rp"], gold[f"{name}_1hop_ci"])
+        for c, (k, iters, rc) in enumerate(gold["kmeans_cases"]):
+            got = oracle.kmeans(h, int(k), int(iters), vs.reference_rand_starts(int(k), 1), bool(rc))
+            np.testing.assert_array_equal(got, gold[f"{name}_kmeans_{c}"], err_msg=f"{name} kmeans {c}")
+        g = vs.Graph(gold[f"{name}_rp"], gold[f"{name}_ci"])
+        for c in gold[f"{name}_pack_cases"]:
+            hop, threads, opt = (int(x) for x in gold["pack_cases"][c][:3])
+            if opt:
+                continue
+            order, offs = vs.packing_order(gold[f"{name}_kmeans_0"], "1x4" if threads == 1 else "4", threads)
+            cap = int(float(gold[f"{name}_pack_{c}_mem"][0]) * 1000 * 1000 * 1000 / 4)
+            bins, nb, sizes = oracle.view_packing(g, order, offs, hop, cap)
+            assert nb == int(gold[f"{name}_pack_{c}_nbins"][0])
+            np.testing.assert_array_equal(bins, gold[f"{name}_pack_{c}_vbmap"], err_msg=f"{name} pack {c}")
+            np.testing.assert_array_equal(sizes, gold[f"{name}_pack_{c}_sizes"], err_msg=f"{name} pack {c}")
+
+
+REF_TOOLS = os.path.join(os.path.dirname(HERE), "oracle", "_ref")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_TOOLS, "view_packing")), reason="the reference's view tools are not built")
+def test_oracle_restatement_equals_reference_tools_on_random_graphs(vs, tmp_path):
+    """Beyond the fixtures: seeded graphs of other shapes, the reference binaries
+    (oracle/_ref) against the restatement, kmeans -t 1 and packing at hop 2 and 3."""
+    import oracle
+    graphs = [vs.gen_rmat(10, 6, seed=s) for s in (21, 22)] + [vs.gen_chung_lu(1500, 7000, g, 120, seed=9) for g in (2.2, 2.7)]
+    for i, g in enumerate(graphs):
+        d = tmp_path / f"g{i}"
+        d.mkdir()
+        vs.write_csr_bin(d / "g.bin", g)
+        subprocess.run([os.path.join(REF_TOOLS, "features"), "-f", "g.bin", "-h", "1", "-t", "1"], cwd=d, check=True, capture_output=True)
+        subprocess.run([os.path.join(REF_TOOLS, "kmeans"), "-f", "g.bin.1hop.bin", "-k", "5", "-i", "4", "-t", "1", "-init", "1"], cwd=d,
+                       check=True, capture_output=True)
+        want = np.loadtxt(d / "g.bin.1hop.bin.kmeans.5", dtype=np.int32)
+        h = vs.read_csr_bin(d / "g.bin.1hop.bin")
+        np.testing.assert_array_equal(oracle.kmeans(h, 5, 4, vs.reference_rand_starts(5, 1)), want)
+        (d / "g.bin.kmeans.1x5").write_bytes((d / "g.bin.1hop.bin.kmeans.5").read_bytes())
+        order, offs = vs.packing_order(want, "1x5", 1)
+        for hop in (2, 3):
+            for frac in (0.05, 0.3, 1.0):
+                mem = frac * g.E * 4 / 1e9
+                cap = int(mem * 1000 * 1000 * 1000 / 4)  # the bin size as the reference derives it from -m
+                try:
+                    bins, nb, _ = oracle.view_packing(g, order, offs, hop, cap)
+                    break
+                except ValueError:
+                    continue
+            r = subprocess.run([os.path.join(REF_TOOLS, "view_packing"), "-gf", "g.bin", "-pf", "g.bin.kmeans.1x5", "-h", str(hop), "-m",
+                                repr(mem), "-t", "1", "-s", "1"], cwd=d, capture_output=True, text=True)
+            assert r.returncode == 0, r.stderr
+            wb, wn = vs.read_vbmap(d / f"g.bin.{hop}.hop.vbmap", g.V)
+            assert nb == wn, (i, hop)
+            np.testing.assert_array_equal(bins, wb, err_msg=f"graph {i} hop {hop}")
