@@ -2276,7 +2276,7 @@ constexpr uint64_t kNoAllocWarps = (uint64_t)kNoAllocBlocks * kDfsWarps;
 constexpr uint64_t kNoAllocMaxTasks = 16384;
 // layout: [0, 256) counters | [256, 1280) plan + view | tasks | per-warp scratch
 constexpr size_t kNoAllocHeader = 256;
-constexpr size_t kNoAllocDescOff = 256;
+constexpr size_t kNoAllocDescOff = kNoAllocHeader;  // the plan and view descriptors follow the counters
 constexpr size_t kNoAllocTaskOff = 1280;
 constexpr size_t kNoAllocScratchOff = (kNoAllocTaskOff + kNoAllocMaxTasks * sizeof(DfsTask) + 255) & ~(size_t)255;
 constexpr uint64_t kNoAllocWarpU32 = (kNoAllocBytes - kNoAllocScratchOff) / (kNoAllocWarps * sizeof(uint32_t));
